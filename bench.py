@@ -1,0 +1,346 @@
+"""Benchmark of the H|psi> drop-in on the Si64 workload (one JSON line on rank 0).
+
+Workload (the configuration the headline metric is quoted on): Si 64-atom
+cubic supercell, a = 20.52 bohr, seeded 0.02 bohr displacements, Ecut 16 Ha
+(26,529 plane waves at Gamma), 96^3 FFT box, 256 KB projectors, 160 bands.
+A step is one H|psi> application to all 160 bands (one hk_psi_c16 call).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value: bands/s of the FP64 drop-in with inputs resident in HBM, summed over
+ranks (replicas, one per GPU), device-timed with CUDA events, L2 flushed
+(256 MiB memset) before every timed step. e2e: the same metric through the
+reference-facing C ABI (cpw_b200_hk_psi_c16) on pinned host arrays, the H2D
+copy of psi and the D2H copy of hpsi inside the timed region. --impl reference
+times the CPU restatement of the reference's hk_psi_c16 (C + OpenMP, all host
+threads) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from cpw2000_b200 import configs  # noqa: E402
+
+METRIC = "H|psi> bands/s"
+NB = 160
+WORKLOAD = "si64"
+
+
+def workload_desc(d):
+    return {"workload": "si64_cubic_ecut16_box96: Si64 cubic a=20.52, sigma 0.02, Ecut 16 Ha, Gamma, "
+                        f"mtxd {d['mtxd']}, box 96^3, {d['nanl']} KB projectors, {NB} bands",
+            "bands": NB, "mtxd": int(d["mtxd"]), "box": [int(v) for v in d["kmscr"][3:6]], "nanl": int(d["nanl"]),
+            "l2": "flushed between timed steps (256 MiB memset); psi+hpsi 136 MB > L2 126 MB"}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), float(j.get("bf16_tflops", 0.0)), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def cpu_reference_rate(d, nbands: int, nthreads: int = 0, repeats: int = 1):
+    """bands/s of the C + OpenMP restatement of hk_psi_c16 on a sample of bands."""
+    from oracle import c_ref
+    psi = configs.random_psi(d["mtxd"], nbands, 1234)
+    args = (d["mtxd"], nbands, psi, d["ekpg"], d["isort"], d["vscr"], d["kmscr"], d["kgv"], d["anlga"], d["xnlkb"])
+    c_ref.hk_psi_c16(*args[:1], 1, psi[:, :1], *args[3:], nthreads=nthreads)     # warm (plans, pages)
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        c_ref.hk_psi_c16(*args, nthreads=nthreads)
+        times.append(time.perf_counter() - t0)
+    return nbands / min(times), (nthreads or c_ref.max_threads())
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    w = configs.si64_cubic()
+    d = configs.kpoint_inputs(w, 0)
+    from oracle import c_ref
+    c_ref.lib()
+    nthreads = c_ref.max_threads()
+    sample = 4
+    for _ in range(args.warmup):
+        cpu_reference_rate(d, sample, nthreads)
+    rates = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r, _ = cpu_reference_rate(d, sample, nthreads)
+        rates.append(r)
+    wall = time.perf_counter() - t0
+    value = statistics.median(rates)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "bands/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sample / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Gaussian pseudopotentials, random complex128 wavefunctions)",
+            "config": {**workload_desc(d), "sample_bands_per_step": sample},
+            "cpu_baseline": {"value": value, "unit": "bands/s", "cores": nthreads, "kind": "port",
+                             "sample": f"{sample} of {NB} bands per step, C+OpenMP restatement of hk_psi_c16 "
+                                       f"(pruned FFT + ZGEMM loops), {nthreads} threads"},
+            "e2e": {"value": value, "unit": "bands/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+    print(json.dumps(line), flush=True)
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1 and args.impl == "ours":
+        import datetime
+
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def run_ours(args, world, rank, local, dist):
+    import torch
+
+    from cpw2000_b200 import _lib
+    from cpw2000_b200 import hk_psi as H
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = configs.si64_cubic()
+    d = configs.kpoint_inputs(w, 0)
+    m = d["mtxd"]
+    psi_h = configs.random_psi(m, NB, 2024 + rank)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    psi = torch.from_numpy(np.ascontiguousarray(psi_h.T)).to(dev).t()
+    hpsi = torch.empty((NB, m), dtype=torch.complex128, device=dev).t()
+
+    def timed(ctx, steps, warmup):
+        for _ in range(warmup):
+            ctx.hk_psi(psi, hpsi)
+        barrier()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        ctx.timing_begin()
+        for a, b in evs:
+            flush.zero_()
+            a.record()
+            ctx.hk_psi(psi, hpsi)
+            b.record()
+        barrier()
+        stages = ctx.timing_end()
+        ms = sum(a.elapsed_time(b) for a, b in evs) / steps
+        return ms, stages
+
+    results = {}
+    sampler = ClockSampler(local)
+    sampler.start()
+    for prec_name, prec in (("fp64", H.FP64), ("mixed", H.MIXED)):
+        ctx = H.Context(local, precision=prec).setup(d)
+        ctx.set_slab_budget(4 << 30)
+        ms, stages = timed(ctx, args.steps, args.warmup)
+        results[prec_name] = (max_over_ranks(ms), stages)
+        ctx.close()
+    clocks = sampler.stop()
+
+    # e2e through the reference-facing C ABI with pinned host arrays
+    psi_pin = torch.from_numpy(np.asfortranarray(psi_h).ravel(order="F").view(np.float64)).pin_memory()
+    hpsi_pin = torch.empty_like(psi_pin).pin_memory()
+    kgv = np.asfortranarray(d["kgv"], dtype=np.int32)
+    isort = np.ascontiguousarray(d["isort"], dtype=np.int32)
+    ekpg = np.ascontiguousarray(d["ekpg"])
+    vscr = np.ascontiguousarray(d["vscr"])
+    kmscr = np.ascontiguousarray(d["kmscr"], dtype=np.int32)
+    anlga = np.asfortranarray(d["anlga"])
+    xnlkb = np.ascontiguousarray(d["xnlkb"])
+    L = _lib.lib()
+    import ctypes as C
+    DP = C.POINTER(C.c_double)
+    pp = C.cast(C.c_void_p(psi_pin.data_ptr()), DP)
+    hp = C.cast(C.c_void_p(hpsi_pin.data_ptr()), DP)
+    ri = _lib.iref
+
+    def dropin(lnew):
+        lv = C.c_int(lnew)
+        st = L.cpw_b200_hk_psi_c16(ri(m), ri(NB), pp, hp, C.byref(lv), ri(d["ng"]), _lib.iptr(kgv),
+                                   _lib.dptr(ekpg), _lib.iptr(isort), _lib.dptr(vscr), _lib.iptr(kmscr),
+                                   _lib.zptr(anlga), _lib.dptr(xnlkb), ri(d["nanl"]), ri(m), ri(NB),
+                                   ri(d["nanl"]), ri(d["ng"]), ri(vscr.size))
+        _lib.check(st)
+
+    dropin(1)
+    for _ in range(args.warmup):
+        dropin(0)
+    barrier()
+    t_e2e = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dropin(0)
+        t_e2e.append(time.perf_counter() - t0)
+    barrier()
+    e2e_ms = max_over_ranks(1e3 * sum(t_e2e) / len(t_e2e))
+
+    ms64, st64 = results["fp64"]
+    msmx, stmx = results["mixed"]
+    value = world * NB / (ms64 / 1e3)
+    hbm, _, peak_kind = measured_peaks()
+    # roofline of the dominant kernel of ours (stage with the largest time share among 0..2)
+    plane = 96 * 96
+    nz = None
+    from cpw2000_b200 import crystal
+    kd = crystal.kd_of_basis(d["kgv"], d["isort"])
+    nz = 2 * kd[2] + 1
+    per_band_bytes = {
+        "inv_xy": 16 * m + nz * plane * 16,
+        "z_vloc": 2 * nz * plane * 16,
+        "fwd_xy": nz * plane * 16 + 2 * 16 * m,
+    }
+    ours = {k: st64[k] for k in ("inv_xy", "z_vloc", "fwd_xy")}
+    dom = max(ours, key=lambda k: ours[k][0])
+    tot_ms, launches = ours[dom]
+    bands_per_launch = NB * args.steps / max(launches, 1)
+    alg = per_band_bytes[dom] * bands_per_launch + (96 ** 3 * 8 if dom == "z_vloc" else 0)
+    avg_launch_s = tot_ms / max(launches, 1) / 1e3
+    achieved = alg / avg_launch_s / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic_si64_fp64.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tj = json.load(f)
+        if dom in tj:
+            traffic = tj[dom]["bytes_per_band"] * bands_per_launch
+    total_stage_ms = sum(v[0] for v in st64.values())
+    line = {
+        "metric": METRIC, "value": value, "unit": "bands/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms64, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Gaussian pseudopotentials, random complex128 wavefunctions)",
+        "config": {**workload_desc(d), "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "precision": "fp64 drop-in (FP64 pruned FFT, cuBLAS ZGEMM projectors)"},
+        "e2e": {"value": world * NB / (e2e_ms / 1e3), "unit": "bands/s", "h2d_bytes_per_step": 16 * m * NB,
+                "d2h_bytes_per_step": 16 * m * NB,
+                "path": "cpw_b200_hk_psi_c16 (drop-in C ABI) on pinned host arrays"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic,
+                     "alg_bytes_per_launch": alg, "avg_launch_ms": avg_launch_s * 1e3},
+        "stages_fp64": {k: {"ms_per_step": v[0] / args.steps, "launches": v[1],
+                            "share": v[0] / total_stage_ms if total_stage_ms else None}
+                        for k, v in st64.items() if v[1]},
+        "mixed": {"value": world * NB / (msmx / 1e3), "ms_per_step": msmx,
+                  "speedup_vs_fp64": ms64 / msmx,
+                  "precision": "FP32 pruned FFT + V_loc, FP64 projector GEMMs",
+                  "stages": {k: v[0] / args.steps for k, v in stmx.items() if v[1]}},
+        "gpu_launches": int(sum(v[1] for k, v in st64.items() if k in ("inv_xy", "z_vloc", "fwd_xy"))),
+        "library_launches": {"cublas_zgemm": int(st64["nl_proj"][1] + st64["nl_expand"][1])},
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1:
+        rate, cores = cpu_reference_rate(d, 4)
+        line["cpu_baseline"] = {"value": rate, "unit": "bands/s", "cores": cores, "kind": "port",
+                                "sample": "4 of 160 bands, C+OpenMP restatement of hk_psi_c16 "
+                                          f"(pruned FFT + ZGEMM loops), {cores} threads"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    args = ap.parse_args()
+    world, rank, local, dist = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank)
+        else:
+            run_ours(args, world, rank, local, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

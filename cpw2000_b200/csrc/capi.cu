@@ -1,0 +1,363 @@
+// extern "C" entry points declared in include/cpw_b200.h.
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/cpw_b200.h"
+#include "context.hpp"
+
+namespace cpwb {
+const char* last_error();
+}
+
+using namespace cpwb;
+
+namespace {
+
+int check_ctx(cpw_b200_ctx* c) { return c ? kOk : fail(kBadArg, "null context"); }
+
+// size_fft of Src/ALFA/size_fft.f90, used for the reference's mxdwrk check.
+void size_fft(const int* kmscr, int ns[3]) {
+  static const int prim[11] = {2, 4, 6, 8, 10, 12, 16, 18, 20, 24, 32};
+  static const int sec[6] = {36, 40, 48, 50, 54, 64};
+  for (int n = 0; n < 3; ++n) {
+    const int need = 2 * kmscr[n] + 1;
+    int v = 0;
+    if (need < 32) {
+      for (int j = 0; j < 11; ++j) {
+        v = prim[j];
+        if (need <= v) break;
+      }
+    } else {
+      const int k = (int)(logf((float)need) / logf(2.0f));
+      for (int j = 0; j < 6; ++j) {
+        v = (1 << (k - 5)) * sec[j];
+        if (need <= v) break;
+      }
+    }
+    ns[n] = v;
+  }
+}
+
+std::mutex g_default_mu;
+cpw_b200_ctx* g_default = nullptr;
+
+int default_ctx(cpw_b200_ctx** out) {
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  if (!g_default) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    int s = cpw_b200_create(&g_default, dev);
+    if (s) return s;
+  }
+  *out = g_default;
+  return kOk;
+}
+
+template <typename T> bool same(const std::vector<T>& v, const T* p, size_t n) {
+  return v.size() == n && (n == 0 || memcmp(v.data(), p, n * sizeof(T)) == 0);
+}
+
+// Copy the leading mtxd rows of ncol complex(8) columns with leading dimension ld.
+int h2d_cols(void* dst, long long ldd, const double* src, long long lds, long long rows, long long cols,
+             cudaStream_t st) {
+  if (rows == 0 || cols == 0) return kOk;
+  cudaError_t e = cudaMemcpy2DAsync(dst, ldd * 16, src, lds * 16, rows * 16, cols, cudaMemcpyHostToDevice, st);
+  return e == cudaSuccess ? kOk : cuda_fail(e, "cudaMemcpy2D H2D");
+}
+int d2h_cols(double* dst, long long ldd, const void* src, long long lds, long long rows, long long cols,
+             cudaStream_t st) {
+  if (rows == 0 || cols == 0) return kOk;
+  cudaError_t e = cudaMemcpy2DAsync(dst, ldd * 16, src, lds * 16, rows * 16, cols, cudaMemcpyDeviceToHost, st);
+  return e == cudaSuccess ? kOk : cuda_fail(e, "cudaMemcpy2D D2H");
+}
+
+[[noreturn]] void stop_like_fortran(const char* routine) {
+  printf("\n   STOPPED in %s:  %s\n", routine, cpwb::last_error());
+  fflush(stdout);
+  exit(1);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cpw_b200_last_error(void) { return cpwb::last_error(); }
+int cpw_b200_version(void) { return 10000; }
+
+int cpw_b200_create(cpw_b200_ctx** out, int device) {
+  if (!out) return fail(kBadArg, "create: null output pointer");
+  *out = nullptr;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  cpw_b200_ctx* c = new cpw_b200_ctx();
+  c->device = device;
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return cuda_fail(e, "cudaStreamCreate");
+  }
+  cublasStatus_t bs = cublasCreate(&c->blas);
+  if (bs != CUBLAS_STATUS_SUCCESS) {
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return fail(kCublas, "cublasCreate failed");
+  }
+  cublasSetStream(c->blas, c->stream);
+  *out = c;
+  return kOk;
+}
+
+int cpw_b200_destroy(cpw_b200_ctx* c) {
+  if (!c) return kOk;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  if (c->blas) cublasDestroy(c->blas);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return kOk;
+}
+
+void* cpw_b200_stream(cpw_b200_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int cpw_b200_synchronize(cpw_b200_ctx* c) {
+  if (int s = check_ctx(c)) return s;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? kOk : cuda_fail(e, "synchronize");
+}
+
+int cpw_b200_set_precision(cpw_b200_ctx* c, int mode) {
+  if (int s = check_ctx(c)) return s;
+  if (mode != CPW_B200_FP64 && mode != CPW_B200_MIXED) return fail(kBadArg, "set_precision: unknown mode");
+  if (mode != c->precision && c->have_basis) {
+    // shared-memory tiling depends on the element size: caller must set the k-point again
+    c->have_basis = false;
+    c->have_pot = false;
+  }
+  c->precision = mode;
+  return kOk;
+}
+
+int cpw_b200_set_slab_budget(cpw_b200_ctx* c, long long bytes) {
+  if (int s = check_ctx(c)) return s;
+  if (bytes <= 0) return fail(kBadArg, "set_slab_budget: bytes must be positive");
+  c->slab_budget = (size_t)bytes;
+  return kOk;
+}
+
+int cpw_b200_timing_begin(cpw_b200_ctx* c) {
+  if (int s = check_ctx(c)) return s;
+  c->timer.on = true;
+  c->timer.used = 0;
+  c->timer.recs.clear();
+  return kOk;
+}
+
+int cpw_b200_timing_end(cpw_b200_ctx* c, double* ms, long long* launches, int nstage) {
+  if (int s = check_ctx(c)) return s;
+  c->timer.on = false;
+  for (int k = 0; k < nstage; ++k) {
+    ms[k] = 0.0;
+    launches[k] = 0;
+  }
+  for (const auto& r : c->timer.recs) {
+    cudaError_t e = cudaEventSynchronize(r.b);
+    if (e != cudaSuccess) return cuda_fail(e, "timing_end");
+    float t = 0.f;
+    e = cudaEventElapsedTime(&t, r.a, r.b);
+    if (e != cudaSuccess) return cuda_fail(e, "timing_end");
+    if (r.stage >= 0 && r.stage < nstage) {
+      ms[r.stage] += t;
+      launches[r.stage] += 1;
+    }
+  }
+  c->timer.recs.clear();
+  c->timer.used = 0;
+  return kOk;
+}
+
+int cpw_b200_set_kpoint(cpw_b200_ctx* c, int mtxd, const int* isort, const int* kgv, int ng, const double* ekpg,
+                        const int* kmscr) {
+  if (int s = check_ctx(c)) return s;
+  cudaSetDevice(c->device);
+  return ctx_set_basis(c, mtxd, isort, kgv, ng, ekpg, kmscr);
+}
+
+int cpw_b200_set_potential(cpw_b200_ctx* c, const double* vscr, long long mxdscr) {
+  if (int s = check_ctx(c)) return s;
+  cudaSetDevice(c->device);
+  return ctx_set_potential(c, vscr, mxdscr);
+}
+
+int cpw_b200_set_projectors(cpw_b200_ctx* c, int nanl, const double* anlga, int mxddim, const double* xnlkb) {
+  if (int s = check_ctx(c)) return s;
+  cudaSetDevice(c->device);
+  return ctx_set_projectors(c, nanl, anlga, mxddim, xnlkb, false);
+}
+
+int cpw_b200_set_projectors_device(cpw_b200_ctx* c, int nanl, const void* anlga, int ld, const void* xnlkb) {
+  if (int s = check_ctx(c)) return s;
+  cudaSetDevice(c->device);
+  return ctx_set_projectors(c, nanl, (const double*)anlga, ld, (const double*)xnlkb, true);
+}
+
+int cpw_b200_hk_psi_device(cpw_b200_ctx* c, int neig, const void* psi, long long ldpsi, void* hpsi, long long ldh,
+                           void* stream) {
+  if (int s = check_ctx(c)) return s;
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  return ctx_hkpsi_device(c, neig, psi, ldpsi, hpsi, ldh, st, true, true);
+}
+
+int cpw_b200_hk_psi_loc_device(cpw_b200_ctx* c, int neig, const void* psi, long long ldpsi, void* hpsi,
+                               long long ldh, void* stream) {
+  if (int s = check_ctx(c)) return s;
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  return ctx_hkpsi_device(c, neig, psi, ldpsi, hpsi, ldh, st, false, false);
+}
+
+int cpw_b200_hk_psi_c16(const int* mtxd, const int* neig, const double* psi, double* hpsi, int* lnewanl,
+                        const int* ng, const int* kgv, const double* ekpg, const int* isort, const double* vscr,
+                        const int* kmscr, const double* anlga, const double* xnlkb, const int* nanl,
+                        const int* mxddim, const int* mxdbnd, const int* mxdanl, const int* mxdgve,
+                        const int* mxdscr) {
+  // argument checks of hk_psi_c16.f90:110-119 plus the array bounds it assumes
+  if (*ng > *mxdgve) return fail(kBadArg, "hk_psi_c16: ng > mxdgve");
+  if (*mtxd < 0 || *mtxd > *mxddim) return fail(kBadArg, "hk_psi_c16: mtxd out of range of mxddim");
+  if (*neig < 0 || *neig > *mxdbnd) return fail(kBadArg, "hk_psi_c16: neig out of range of mxdbnd");
+  if (*nanl < 0 || *nanl > *mxdanl) return fail(kBadArg, "hk_psi_c16: nanl out of range of mxdanl");
+  {
+    int ns[3];
+    size_fft(kmscr, ns);
+    const long long mxdwrk =
+        4LL * std::max((long long)ns[0] * ns[1], std::max((long long)ns[0] * ns[2], (long long)ns[1] * ns[2]));
+    if (mxdwrk > *mxdscr) {
+      char buf[160];
+      snprintf(buf, sizeof buf, "hk_psi_c16: mxdwrk = %lld is greater than mxdscr = %d", mxdwrk, *mxdscr);
+      return fail(kBadArg, buf);
+    }
+    if ((long long)kmscr[6] * kmscr[4] * kmscr[5] > *mxdscr)
+      return fail(kBadArg, "hk_psi_c16: vscr (mxdscr) smaller than id*n2*n3");
+  }
+  cpw_b200_ctx* c;
+  if (int s = default_ctx(&c)) return s;
+  cudaSetDevice(c->device);
+  const int m = *mtxd, nb = *neig;
+  // k-point arrays: re-upload when any of them changed
+  std::vector<int> kg((size_t)3 * m);
+  for (int i = 0; i < m; ++i) {
+    const int it = isort[i];
+    if (it < 1 || it > *ng) return fail(kBadArg, "hk_psi_c16: isort out of range");
+    for (int j = 0; j < 3; ++j) kg[3 * (size_t)i + j] = kgv[3 * (size_t)(it - 1) + j];
+  }
+  bool kchanged = !c->have_basis || c->sh_mtxd != m || !same(c->sh_kmscr, kmscr, 7) ||
+                  !same(c->sh_isort, isort, (size_t)m) || !same(c->sh_kgv, kg.data(), kg.size()) ||
+                  !same(c->sh_ekpg, ekpg, (size_t)m);
+  int s;
+  if (kchanged) {
+    // the compact kgv(3, mtxd) of the basis with isort = 1..mtxd is what the device needs
+    std::vector<int> iota(m);
+    for (int i = 0; i < m; ++i) iota[i] = i + 1;
+    if ((s = ctx_set_basis(c, m, iota.data(), kg.data(), m, ekpg, kmscr))) return s;
+    c->sh_mtxd = m;
+    c->sh_kmscr.assign(kmscr, kmscr + 7);
+    c->sh_isort.assign(isort, isort + m);
+    c->sh_kgv = kg;
+    c->sh_ekpg.assign(ekpg, ekpg + m);
+    c->sh_vscr.clear();
+  }
+  const size_t nv = (size_t)kmscr[6] * kmscr[4] * kmscr[5];
+  if (!c->have_pot || !same(c->sh_vscr, vscr, nv)) {
+    if ((s = ctx_set_potential(c, vscr, *mxdscr))) return s;
+    c->sh_vscr.assign(vscr, vscr + nv);
+  }
+  if (kchanged || *lnewanl != 0 || c->nanl != *nanl) {
+    if ((s = ctx_set_projectors(c, *nanl, anlga, *mxddim, xnlkb, false))) return s;
+    *lnewanl = 0;
+  }
+  if (m == 0 || nb == 0) return kOk;
+  const size_t bytes = (size_t)m * nb * 16;
+  if ((s = c->h_in.ensure(bytes))) return s;
+  if ((s = c->h_out.ensure(bytes))) return s;
+  if ((s = h2d_cols(c->h_in.p, m, psi, *mxddim, m, nb, c->stream))) return s;
+  if ((s = ctx_hkpsi_device(c, nb, c->h_in.p, m, c->h_out.p, m, c->stream, true, true))) return s;
+  if ((s = d2h_cols(hpsi, *mxddim, c->h_out.p, m, m, nb, c->stream))) return s;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? kOk : cuda_fail(e, "hk_psi_c16");
+}
+
+void hk_psi_c16_(const int* mtxd, const int* neig, const double* psi, double* hpsi, int* lnewanl, const int* ng,
+                 const int* kgv, const double* ekpg, const int* isort, const double* vscr, const int* kmscr,
+                 const double* anlga, const double* xnlkb, const int* nanl, const int* mxddim, const int* mxdbnd,
+                 const int* mxdanl, const int* mxdgve, const int* mxdscr) {
+  int s = cpw_b200_hk_psi_c16(mtxd, neig, psi, hpsi, lnewanl, ng, kgv, ekpg, isort, vscr, kmscr, anlga, xnlkb, nanl,
+                              mxddim, mxdbnd, mxdanl, mxdgve, mxdscr);
+  if (s) stop_like_fortran("hk_psi_c16");
+}
+
+int cpw_b200_hk_psi_nl_c16(const int* mtxd, const int* neig, const double* psi, double* hpsi, const double* anlga,
+                           const double* xnlkb, const int* nanl, const int* ladd, const int* mxddim,
+                           const int* mxdbnd, const int* mxdanl) {
+  if (*mtxd < 0 || *mtxd > *mxddim) return fail(kBadArg, "hk_psi_nl_c16: mtxd out of range of mxddim");
+  if (*neig < 0 || *neig > *mxdbnd) return fail(kBadArg, "hk_psi_nl_c16: neig out of range of mxdbnd");
+  if (*nanl < 0 || *nanl > *mxdanl) return fail(kBadArg, "hk_psi_nl_c16: nanl out of range of mxdanl");
+  const int m = *mtxd, nb = *neig, na = *nanl;
+  if (m == 0 || nb == 0) return kOk;
+  cpw_b200_ctx* c;
+  if (int s = default_ctx(&c)) return s;
+  cudaSetDevice(c->device);
+  DevBuf x, xd, p, h, v;
+  int s;
+  if (na == 0) {
+    if (*ladd == 0) {
+      for (int n = 0; n < nb; ++n) memset(hpsi + 2 * (size_t)n * *mxddim, 0, (size_t)m * 16);
+    }
+    return kOk;
+  }
+  if ((s = h.ensure((size_t)m * nb * 16)) || (s = x.ensure((size_t)m * na * 16)) || (s = p.ensure((size_t)na * nb * 16)) ||
+      (s = v.ensure((size_t)m * nb * 16)) || (s = xd.ensure((size_t)na * 8)))
+    return s;
+  if ((s = h2d_cols(x.p, m, anlga, *mxddim, m, na, c->stream))) return s;
+  if ((s = h2d_cols(v.p, m, psi, *mxddim, m, nb, c->stream))) return s;
+  if (*ladd) {
+    if ((s = h2d_cols(h.p, m, hpsi, *mxddim, m, nb, c->stream))) return s;
+  }
+  cudaMemcpyAsync(xd.p, xnlkb, (size_t)na * 8, cudaMemcpyHostToDevice, c->stream);
+  cublasSetStream(c->blas, c->stream);
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+  cublasStatus_t bs = cublasZgemm(c->blas, CUBLAS_OP_C, CUBLAS_OP_N, na, nb, m, &one, (const cuDoubleComplex*)x.p,
+                                  m, (const cuDoubleComplex*)v.p, m, &zero, (cuDoubleComplex*)p.p, na);
+  if (bs != CUBLAS_STATUS_SUCCESS) return fail(kCublas, "hk_psi_nl_c16: zgemm 'c','n'");
+  // dhd := Diag(xnlkb) dhd (hk_psi_nl_c16.f90:87-91) as a row scaling of P
+  {
+    std::vector<double> dz(2 * (size_t)na, 0.0);
+    for (int i = 0; i < na; ++i) dz[2 * (size_t)i] = xnlkb[i];
+    DevBuf dd;
+    if ((s = dd.ensure(dz.size() * 8))) return s;
+    cudaMemcpyAsync(dd.p, dz.data(), dz.size() * 8, cudaMemcpyHostToDevice, c->stream);
+    bs = cublasZdgmm(c->blas, CUBLAS_SIDE_LEFT, na, nb, (const cuDoubleComplex*)p.p, na,
+                     (const cuDoubleComplex*)dd.p, 1, (cuDoubleComplex*)p.p, na);
+    if (bs != CUBLAS_STATUS_SUCCESS) return fail(kCublas, "hk_psi_nl_c16: zdgmm");
+    const cuDoubleComplex beta = *ladd ? one : zero;
+    bs = cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, m, nb, na, &one, (const cuDoubleComplex*)x.p, m,
+                     (const cuDoubleComplex*)p.p, na, &beta, (cuDoubleComplex*)h.p, m);
+    if (bs != CUBLAS_STATUS_SUCCESS) return fail(kCublas, "hk_psi_nl_c16: zgemm 'n','n'");
+    if ((s = d2h_cols(hpsi, *mxddim, h.p, m, m, nb, c->stream))) return s;
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "hk_psi_nl_c16");
+  }
+  return kOk;
+}
+
+void hk_psi_nl_c16_(const int* mtxd, const int* neig, const double* psi, double* hpsi, const double* anlga,
+                    const double* xnlkb, const int* nanl, const int* ladd, const int* mxddim, const int* mxdbnd,
+                    const int* mxdanl) {
+  int s = cpw_b200_hk_psi_nl_c16(mtxd, neig, psi, hpsi, anlga, xnlkb, nanl, ladd, mxddim, mxdbnd, mxdanl);
+  if (s) stop_like_fortran("hk_psi_nl_c16");
+}
+
+}  // extern "C"

@@ -1,0 +1,99 @@
+// Per-k-point device state shared by the H|psi> and eigensolver entry points.
+#pragma once
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "hkpsi_local.cuh"
+
+struct cpw_b200_ctx;
+
+namespace cpwb {
+
+// Status codes of the C ABI (also in include/cpw_b200.h).
+enum Status : int {
+  kOk = 0,
+  kBadArg = 1,        // invalid dimension / argument (the reference would stop)
+  kWrap = 2,          // basis wraps around the FFT box (hk_psi_c16.f90:161-172)
+  kUnsupported = 3,   // FFT length not factorable into supported radices, or too large
+  kNotReady = 4,      // basis / potential not set
+  kNotConverged = 5,  // eigensolver: see ifail
+  kCuda = -1,         // CUDA runtime error
+  kCublas = -2,       // cuBLAS error
+  kCusolver = -3,     // cuSOLVER error
+  kTimeout = -4,      // a bounded device wait gave up
+};
+
+// Stage timers: CUDA events recorded around every kernel of a stage while
+// enabled; read back (with one synchronisation) by timing_end.
+enum Stage : int { kStInvXY = 0, kStZVloc = 1, kStFwdXY = 2, kStNlProj = 3, kStNlExpand = 4, kStEig = 5, kNumStages = 8 };
+struct StageTimer {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  struct Rec { int stage; cudaEvent_t a, b; };
+  std::vector<Rec> recs;
+  cudaEvent_t take();                       // nullptr when the pool is exhausted
+  void mark(int stage, cudaEvent_t a, cudaEvent_t b) { if (a && b) recs.push_back({stage, a, b}); }
+  ~StageTimer();
+};
+
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  int ensure(size_t need);
+  void release();
+  ~DevBuf() { release(); }
+};
+
+}  // namespace cpwb
+
+struct cpw_b200_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cublasHandle_t blas = nullptr;
+  int precision = 0;            // 0: FP64 local + FP64 projector GEMMs; 1: FP32 local (mixed)
+  size_t slab_budget = 512ull << 20;
+
+  // basis of the current k-point
+  bool have_basis = false;
+  int mtxd = 0;
+  int ident = 0;                // leading dimension id of the reference box (kmscr(7))
+  cpwb::LocalPlan plan{};
+  cpwb::DevBuf plane_start, pw_idx, pw_pos, ekpg;
+  cpwb::DevBuf tw64[3], tw32[3];
+
+  // local potential on the box, [z][y][x] scaled by 1/N
+  bool have_pot = false;
+  int pot_n[3] = {0, 0, 0};
+  cpwb::DevBuf v64, v32;
+
+  // KB projectors (column-major mtxd x nanl) pre-multiplied by xnlkb in anld
+  int nanl = 0;
+  cpwb::DevBuf anl, anld, proj;
+
+  cpwb::StageTimer timer;
+
+  // slab for the band chunk and staging for host-array entry points
+  cpwb::DevBuf slab, h_in, h_out;
+
+  // host shadows used by the drop-in to decide what to re-upload
+  std::vector<int> sh_isort, sh_kgv, sh_kmscr;
+  std::vector<double> sh_ekpg, sh_vscr;
+  int sh_mtxd = -1;
+};
+
+namespace cpwb {
+int ctx_set_basis(cpw_b200_ctx* c, int mtxd, const int* isort, const int* kgv, int ng, const double* ekpg,
+                  const int* kmscr);
+int ctx_set_potential(cpw_b200_ctx* c, const double* vscr, long long nscr);
+int ctx_set_projectors(cpw_b200_ctx* c, int nanl, const double* anlga, int ld, const double* xnlkb, bool on_device);
+int ctx_hkpsi_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh,
+                     cudaStream_t st, bool with_kinetic, bool with_nl);
+}  // namespace cpwb

@@ -1,0 +1,68 @@
+// Local part of H|psi>: G-sphere scatter, pruned inverse 3D FFT, V_loc(r)
+// multiply, pruned forward 3D FFT, gather and kinetic diagonal, for a chunk
+// of bands. Restates the per-band loop of Src/hk_psi/reference/hk_psi_c16.f90
+// (:176-223) with the Goedecker pruning of Src/fft/_cfft/cfft_wf_c16.f
+// (:110-410), re-organised for the GPU as three kernels per band chunk:
+//
+//   A  one CTA per (band, kept z-plane): scatter the plane's coefficients
+//      into shared memory, inverse FFT along x on the 2kd2+1 kept rows,
+//      inverse FFT along y on every column, write the plane to the slab W.
+//   B  one CTA per (band, run of xy columns): inverse FFT along z of the
+//      2kd3+1 kept planes, multiply by V(r)/N, forward FFT along z, keep the
+//      2kd3+1 planes. The inverse's second pass, the multiply and the
+//      forward's first pass share registers.
+//   C  one CTA per (band, kept z-plane): forward FFT along y keeping the kept
+//      rows, forward FFT along x, gather the sphere, add ekpg*psi.
+//
+// Slab W layout: [band][zi][y][x] (x fastest), zi = compact index of the
+// kept z planes. Every 1D transform of length n = r1*r2 is two register
+// passes with one shared-memory exchange (four-step), twiddles W_n^k from a
+// table in shared memory.
+#pragma once
+#include "cplx.cuh"
+
+namespace cpwb {
+
+struct FftDim {
+  int n, r1, r2;
+};
+
+struct LocalPlan {
+  int n1, n2, n3;         // FFT box
+  int kd1, kd2, kd3;      // sphere half-widths (largest |k_j| of the basis)
+  int nx, ny, nz;         // 2*kd+1
+  FftDim dx, dy, dz;
+  int rowp;               // shared-memory row stride (complex elements) in A/C
+  int tcol;               // columns per batch in the y passes of A/C
+  int cb;                 // columns per CTA in B
+  long long plane;        // n1*n2
+};
+
+__host__ __device__ __forceinline__ int kept_to_idx(int i, int kd, int n, int nk) {
+  return i <= kd ? i : n - nk + i;
+}
+__host__ __device__ __forceinline__ int idx_to_kept(int z, int kd, int n, int nk) {
+  return z <= kd ? z : (z >= n - kd ? z - (n - nk) : -1);
+}
+
+// Shared-memory footprint in bytes of kernels A/C and B.
+template <typename T> inline size_t smem_planes(const LocalPlan& p) {
+  return sizeof(C2<T>) * ((size_t)p.ny * p.rowp + (size_t)p.n2 * p.tcol + p.n1 + p.n2);
+}
+template <typename T> inline size_t smem_columns(const LocalPlan& p) {
+  return sizeof(C2<T>) * ((size_t)p.n3 * p.cb + p.n3);
+}
+
+// Launch the three kernels for bands [band0, band0+nbc). psi/hpsi are
+// complex128 column-major with leading dimensions ldpsi/ldh. W holds nbc
+// slabs. ekpg may be null (no kinetic term). If ev is not null, ev[0..3] are
+// recorded before A, after A, after B and after C (stage timers). Returns a
+// cudaError_t.
+template <typename T>
+cudaError_t launch_local(const LocalPlan& p, int nbc, int band0, const C2<double>* psi, long long ldpsi,
+                         C2<double>* hpsi, long long ldh, const int* plane_start, const int* pw_idx,
+                         const int* pw_pos, const double* ekpg, const T* vr, const C2<T>* twx,
+                         const C2<T>* twy, const C2<T>* twz, C2<T>* W, cudaStream_t st,
+                         cudaEvent_t* ev = nullptr);
+
+}  // namespace cpwb

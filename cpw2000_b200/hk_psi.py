@@ -1,0 +1,194 @@
+"""Python mirror of cpw2000's H|psi> interface over the C ABI.
+
+``hk_psi_c16`` / ``hk_psi_nl_c16`` take the reference's argument lists
+(Src/hk_psi/reference/hk_psi_c16.f90:28-32, Src/cpw_lib/hk_psi_nl_c16.f90:23-24)
+with numpy arrays in Fortran order and host memory, like the Fortran callers.
+``Context`` is the device-resident form used by the eigensolver and the
+benchmarks: per-k-point inputs are uploaded once, H|psi> runs on torch CUDA
+tensors (torch supplies the device memory and streams; the compute is the
+library's CUDA kernels).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, dptr, iptr, zptr
+
+FP64 = 0
+MIXED = 1
+
+
+def _as_f(a, dtype):
+    a = np.asarray(a)
+    if a.dtype != dtype or not (a.flags.f_contiguous or a.ndim == 1):
+        a = np.asfortranarray(a, dtype=dtype)
+    return a
+
+
+def hk_psi_c16(mtxd, neig, psi, hpsi, lnewanl, ng, kgv, ekpg, isort, vscr, kmscr, anlga, xnlkb, nanl,
+               mxddim, mxdbnd, mxdanl, mxdgve, mxdscr):
+    """hpsi(:mtxd, :neig) = H psi, as hk_psi_c16 (psi, hpsi: complex128 (mxddim, mxdbnd)).
+
+    ``hpsi`` must be a Fortran-ordered complex128 array; it is written in place
+    and also returned, with the updated ``lnewanl`` (cleared once the library
+    has taken the new projectors). Errors raise ``CpwB200Error`` (the
+    reference stops the program).
+    """
+    L = _lib.lib()
+    psi = _as_f(psi, np.complex128)
+    if not (isinstance(hpsi, np.ndarray) and hpsi.dtype == np.complex128 and hpsi.flags.f_contiguous):
+        raise TypeError("hpsi must be a Fortran-ordered complex128 numpy array (written in place)")
+    if psi.shape[0] < mxddim or hpsi.shape[0] < mxddim:
+        raise ValueError("psi/hpsi leading dimension smaller than mxddim")
+    kgv = _as_f(kgv, np.int32)
+    isort = _as_f(isort, np.int32)
+    ekpg = _as_f(ekpg, np.float64)
+    vscr = _as_f(vscr, np.float64)
+    kmscr = _as_f(kmscr, np.int32)
+    anlga = _as_f(anlga, np.complex128) if nanl > 0 else np.zeros((max(mxddim, 1), 1), np.complex128, order="F")
+    xnlkb = _as_f(xnlkb, np.float64) if nanl > 0 else np.zeros(1)
+    lnew = C.c_int(1 if lnewanl else 0)
+    ri = _lib.iref
+    st = L.cpw_b200_hk_psi_c16(ri(mtxd), ri(neig), zptr(psi), zptr(hpsi),
+                               C.byref(lnew), ri(ng), iptr(kgv), dptr(ekpg), iptr(isort), dptr(vscr), iptr(kmscr),
+                               zptr(anlga), dptr(xnlkb), ri(nanl), ri(mxddim), ri(mxdbnd),
+                               ri(mxdanl), ri(mxdgve), ri(mxdscr))
+    check(st)
+    return hpsi, bool(lnew.value)
+
+
+def hk_psi_nl_c16(mtxd, neig, psi, hpsi, anlga, xnlkb, nanl, ladd, mxddim, mxdbnd, mxdanl):
+    """hpsi = [hpsi if ladd] + anlga diag(xnlkb) anlga^H psi, as hk_psi_nl_c16 (in place)."""
+    L = _lib.lib()
+    psi = _as_f(psi, np.complex128)
+    if not (isinstance(hpsi, np.ndarray) and hpsi.dtype == np.complex128 and hpsi.flags.f_contiguous):
+        raise TypeError("hpsi must be a Fortran-ordered complex128 numpy array (updated in place)")
+    anlga = _as_f(anlga, np.complex128) if nanl > 0 else np.zeros((max(mxddim, 1), 1), np.complex128, order="F")
+    xnlkb = _as_f(xnlkb, np.float64) if nanl > 0 else np.zeros(1)
+    ri = _lib.iref
+    check(L.cpw_b200_hk_psi_nl_c16(ri(mtxd), ri(neig), zptr(psi), zptr(hpsi),
+                                   zptr(anlga), dptr(xnlkb), ri(nanl), ri(1 if ladd else 0),
+                                   ri(mxddim), ri(mxdbnd), ri(mxdanl)))
+    return hpsi
+
+
+class Context:
+    """One k-point's device state; H|psi> on device-resident complex128 torch tensors."""
+
+    def __init__(self, device: int = 0, precision: int = FP64):
+        self._L = _lib.lib()
+        h = C.c_void_p()
+        check(self._L.cpw_b200_create(C.byref(h), int(device)))
+        self.handle = h
+        self.device = device
+        self.mtxd = 0
+        self.nanl = 0
+        if precision != FP64:
+            self.set_precision(precision)
+
+    def close(self):
+        if self.handle:
+            self._L.cpw_b200_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream_ptr(self) -> int:
+        return int(self._L.cpw_b200_stream(self.handle) or 0)
+
+    def set_precision(self, mode: int):
+        check(self._L.cpw_b200_set_precision(self.handle, int(mode)))
+
+    def set_slab_budget(self, nbytes: int):
+        check(self._L.cpw_b200_set_slab_budget(self.handle, int(nbytes)))
+
+    STAGES = ("inv_xy", "z_vloc", "fwd_xy", "nl_proj", "nl_expand", "eig", "s6", "s7")
+
+    def timing_begin(self):
+        check(self._L.cpw_b200_timing_begin(self.handle))
+
+    def timing_end(self) -> dict:
+        """Per-stage {name: (total_ms, launches)} since timing_begin (synchronises)."""
+        ms = (C.c_double * 8)()
+        nl = (C.c_longlong * 8)()
+        check(self._L.cpw_b200_timing_end(self.handle, ms, nl, 8))
+        return {n: (float(ms[i]), int(nl[i])) for i, n in enumerate(self.STAGES)}
+
+    def set_kpoint(self, mtxd, isort, kgv, ekpg, kmscr):
+        isort = np.ascontiguousarray(isort, dtype=np.int32)
+        kgv = np.asfortranarray(kgv, dtype=np.int32)
+        ekpg = np.ascontiguousarray(ekpg, dtype=np.float64)
+        kmscr = np.ascontiguousarray(kmscr, dtype=np.int32)
+        check(self._L.cpw_b200_set_kpoint(self.handle, int(mtxd), iptr(isort), iptr(kgv), int(kgv.shape[1]),
+                                          dptr(ekpg), iptr(kmscr)))
+        self.mtxd = int(mtxd)
+
+    def set_potential(self, vscr):
+        v = np.ascontiguousarray(vscr, dtype=np.float64)
+        check(self._L.cpw_b200_set_potential(self.handle, dptr(v), int(v.size)))
+
+    def set_projectors(self, anlga, xnlkb):
+        a = np.asfortranarray(anlga, dtype=np.complex128)
+        x = np.ascontiguousarray(xnlkb, dtype=np.float64)
+        nanl = int(x.size)
+        if nanl == 0:
+            a = np.zeros((max(self.mtxd, 1), 1), np.complex128, order="F")
+            x = np.zeros(1)
+        check(self._L.cpw_b200_set_projectors(self.handle, nanl, zptr(a), int(a.shape[0]),
+                                              dptr(x)))
+        self.nanl = nanl
+
+    def setup(self, inputs: dict):
+        """Upload one k-point from a dict as returned by configs.kpoint_inputs."""
+        self.set_kpoint(inputs["mtxd"], inputs["isort"], inputs["kgv"], inputs["ekpg"], inputs["kmscr"])
+        self.set_potential(inputs["vscr"])
+        self.set_projectors(inputs["anlga"], inputs["xnlkb"])
+        return self
+
+    @staticmethod
+    def _ld(t) -> int:
+        # column-major (mtxd, nb) stored as torch (nb, ld) row-major or a Fortran view
+        if t.dim() != 2:
+            raise ValueError("expected a 2-D complex128 tensor")
+        if t.stride(0) == 1:
+            return int(t.stride(1))
+        raise ValueError("tensor must be column-major (use .t() of a contiguous (nb, ld) tensor)")
+
+    def hk_psi(self, psi, hpsi, neig=None, stream=None, local_only=False):
+        """hpsi[:, :neig] = H psi[:, :neig] for column-major complex128 CUDA tensors (mtxd rows)."""
+        import torch
+        if psi.dtype != torch.complex128 or hpsi.dtype != torch.complex128:
+            raise TypeError("psi/hpsi must be complex128")
+        if not (psi.is_cuda and hpsi.is_cuda):
+            raise TypeError("psi/hpsi must be CUDA tensors")
+        nb = psi.shape[1] if neig is None else int(neig)
+        s = stream if stream is not None else torch_stream_handle(psi.device)
+        fn = self._L.cpw_b200_hk_psi_loc_device if local_only else self._L.cpw_b200_hk_psi_device
+        check(fn(self.handle, nb, C.c_void_p(psi.data_ptr()), self._ld(psi), C.c_void_p(hpsi.data_ptr()),
+                 self._ld(hpsi), C.c_void_p(s)))
+        return hpsi
+
+
+def torch_stream_handle(device=None) -> int:
+    """cudaStream_t of torch's current stream; the legacy default stream (handle 0)
+    is passed as cudaStreamLegacy, because a null stream means "the context's
+    own stream" to the C ABI."""
+    import torch
+    h = int(torch.cuda.current_stream(device).cuda_stream)
+    return h if h != 0 else CUDA_STREAM_LEGACY
+
+
+CUDA_STREAM_LEGACY = 0x1
+
+
+def colmajor(t):
+    """A (rows, cols) column-major view of a contiguous (cols, rows) tensor."""
+    return t.t()

@@ -1,0 +1,124 @@
+/*
+ * cpw_b200.h -- C ABI of the B200-native H|psi> operator and block eigensolver
+ * for cpw2000 (plain pointers and sizes; no torch or CUDA types in signatures).
+ *
+ * Two layers:
+ *
+ *  1. Drop-ins with the reference's Fortran argument lists, every argument by
+ *     reference as gfortran passes it (LOGICAL is a 4-byte int, 0 = .FALSE.),
+ *     complex(8) arrays as interleaved (re, im) doubles, column-major with the
+ *     reference's leading dimensions, 1-based isort into kgv(3, mxdgve):
+ *       cpw_b200_hk_psi_c16  / hk_psi_c16_    replaces Src/hk_psi/reference/hk_psi_c16.f90:28-32
+ *       cpw_b200_hk_psi_nl_c16 / hk_psi_nl_c16_ replaces Src/cpw_lib/hk_psi_nl_c16.f90:23-24
+ *     The cpw_b200_* forms return a status (0 = success) and never stop the
+ *     program; the trailing-underscore forms are link-time substitutes for the
+ *     Fortran symbols and, like the reference, print the message and stop the
+ *     program on an error (exit status 1).
+ *
+ *  2. A context API for callers that keep data on the device: the per-k-point
+ *     inputs are set once (basis, potential, projectors) and H|psi> is applied
+ *     to device-resident column-major complex128 blocks on a caller stream.
+ *
+ * Threading: a context is not re-entrant; one context per host thread. The
+ * drop-ins use one process-wide context on the current CUDA device and are
+ * synchronous (results are in the host arrays on return), as the reference's
+ * routines are.
+ */
+#ifndef CPW_B200_H
+#define CPW_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define CPW_B200_OK 0
+#define CPW_B200_BAD_ARG 1       /* invalid dimension or argument (the reference stops) */
+#define CPW_B200_WRAP 2          /* basis wraps around the FFT box (hk_psi_c16.f90:161-172) */
+#define CPW_B200_UNSUPPORTED 3   /* FFT length not a product of two radices <= 16, or too large */
+#define CPW_B200_NOT_READY 4     /* context: basis / potential not set */
+#define CPW_B200_NOT_CONVERGED 5 /* eigensolver did not reach epspsi; ifail holds the digits */
+#define CPW_B200_CUDA_ERROR (-1)
+#define CPW_B200_CUBLAS_ERROR (-2)
+#define CPW_B200_CUSOLVER_ERROR (-3)
+#define CPW_B200_TIMEOUT (-4)
+
+/* ---- precision modes ---- */
+#define CPW_B200_FP64 0  /* plain FP64 everywhere (the drop-in default) */
+#define CPW_B200_MIXED 1 /* FP32 FFT/V_loc; projector GEMMs and subspace steps per the mixed form */
+
+typedef struct cpw_b200_ctx cpw_b200_ctx;
+
+/* Message of the last failing call on this host thread ("" if none). */
+const char* cpw_b200_last_error(void);
+/* Library ABI version (major*10000 + minor*100 + patch). */
+int cpw_b200_version(void);
+
+/* ---- context API ---- */
+int cpw_b200_create(cpw_b200_ctx** ctx, int device);
+int cpw_b200_destroy(cpw_b200_ctx* ctx);
+/* The context's own CUDA stream (cudaStream_t as void*). */
+void* cpw_b200_stream(cpw_b200_ctx* ctx);
+int cpw_b200_synchronize(cpw_b200_ctx* ctx);
+int cpw_b200_set_precision(cpw_b200_ctx* ctx, int mode);
+/* Device bytes the FFT slab of one band chunk may use (default 512 MiB). */
+int cpw_b200_set_slab_budget(cpw_b200_ctx* ctx, long long bytes);
+
+/* Stage timers (CUDA events around each kernel of a stage, on the stream the
+ * kernel runs on). timing_end synchronises and writes per-stage totals in ms
+ * and launch counts for stages 0..nstage-1: 0 scatter+inverse xy, 1 inverse z +
+ * V_loc + forward z, 2 forward xy + gather, 3 projection X^H psi, 4 expansion
+ * hpsi += X D P, 5 eigensolver subspace work. */
+int cpw_b200_timing_begin(cpw_b200_ctx* ctx);
+int cpw_b200_timing_end(cpw_b200_ctx* ctx, double* ms, long long* launches, int nstage);
+
+/* Basis of one k-point: isort(mtxd) 1-based into kgv(3, ng), ekpg(mtxd) in
+ * Hartree, kmscr(7) as the reference (kmscr(4:6) = n1,n2,n3, kmscr(7) = id).
+ * Host arrays. (Inputs of hk_psi_c16.f90:28-32 that depend only on k.) */
+int cpw_b200_set_kpoint(cpw_b200_ctx* ctx, int mtxd, const int* isort, const int* kgv, int ng,
+                        const double* ekpg, const int* kmscr);
+/* Screened potential vscr(id*n2*n3) on the FFT box, host array. */
+int cpw_b200_set_potential(cpw_b200_ctx* ctx, const double* vscr, long long mxdscr);
+/* KB projectors anlga(mxddim, nanl) complex(8) and xnlkb(nanl), host arrays
+ * (the outputs of Src/omp/proj_nl_kb_c16.f90). */
+int cpw_b200_set_projectors(cpw_b200_ctx* ctx, int nanl, const double* anlga, int mxddim, const double* xnlkb);
+/* Same with device pointers (anlga complex128, leading dimension ld). */
+int cpw_b200_set_projectors_device(cpw_b200_ctx* ctx, int nanl, const void* anlga, int ld, const void* xnlkb);
+
+/* hpsi = H psi for neig device-resident complex128 columns (ld >= mtxd), on
+ * `stream` (cudaStream_t; NULL = the context stream). Asynchronous.
+ * Same operator as hk_psi_c16.f90:176-231. */
+int cpw_b200_hk_psi_device(cpw_b200_ctx* ctx, int neig, const void* psi, long long ldpsi, void* hpsi,
+                           long long ldhpsi, void* stream);
+/* Local part only, hpsi = V_loc psi (Src/omp/hk_psi_loc_c16.f90 with ladd = .false., nsp = 1). */
+int cpw_b200_hk_psi_loc_device(cpw_b200_ctx* ctx, int neig, const void* psi, long long ldpsi, void* hpsi,
+                               long long ldhpsi, void* stream);
+
+/* ---- drop-ins with the reference argument lists ---- */
+
+/* Src/hk_psi/reference/hk_psi_c16.f90:28-32. lnewanl != 0 tells the library
+ * that anlga/xnlkb were recomputed; it re-uploads them and sets *lnewanl = 0.
+ * The k-point arrays and vscr are compared with the previous call's and
+ * re-uploaded only when they changed. */
+int cpw_b200_hk_psi_c16(const int* mtxd, const int* neig, const double* psi, double* hpsi, int* lnewanl,
+                        const int* ng, const int* kgv, const double* ekpg, const int* isort, const double* vscr,
+                        const int* kmscr, const double* anlga, const double* xnlkb, const int* nanl,
+                        const int* mxddim, const int* mxdbnd, const int* mxdanl, const int* mxdgve,
+                        const int* mxdscr);
+void hk_psi_c16_(const int* mtxd, const int* neig, const double* psi, double* hpsi, int* lnewanl, const int* ng,
+                 const int* kgv, const double* ekpg, const int* isort, const double* vscr, const int* kmscr,
+                 const double* anlga, const double* xnlkb, const int* nanl, const int* mxddim, const int* mxdbnd,
+                 const int* mxdanl, const int* mxdgve, const int* mxdscr);
+
+/* Src/cpw_lib/hk_psi_nl_c16.f90:23-24: hpsi = [hpsi if ladd] + anlga xnlkb anlga^H psi. */
+int cpw_b200_hk_psi_nl_c16(const int* mtxd, const int* neig, const double* psi, double* hpsi, const double* anlga,
+                           const double* xnlkb, const int* nanl, const int* ladd, const int* mxddim,
+                           const int* mxdbnd, const int* mxdanl);
+void hk_psi_nl_c16_(const int* mtxd, const int* neig, const double* psi, double* hpsi, const double* anlga,
+                    const double* xnlkb, const int* nanl, const int* ladd, const int* mxddim, const int* mxdbnd,
+                    const int* mxdanl);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CPW_B200_H */

@@ -1,0 +1,167 @@
+"""GPU parity of H|psi> (C ABI -> sm_100a kernels) against the CPU oracle.
+
+FP64 path: relative error <= 1e-12 of max|H psi| (rounding only; the GPU
+pruned FFT and numpy's FFT differ in operation order). Mixed path (FP32
+FFT/V_loc): relative error <= 2e-5.
+"""
+import numpy as np
+import pytest
+
+from cpw2000_b200 import configs
+from cpw2000_b200 import hk_psi as H
+from cpw2000_b200._lib import CpwB200Error
+from oracle import hk_psi as O
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 2e-5
+
+
+def oracle_hpsi(d, psi, nb):
+    return O.hk_psi_c16(d["mtxd"], nb, psi, d["ekpg"], d["isort"], d["vscr"], d["kmscr"], d["kgv"], d["anlga"],
+                        d["xnlkb"])
+
+
+def to_dev(a, torch, dev):
+    # column-major complex128 (rows, cols) on the device
+    return torch.from_numpy(np.ascontiguousarray(a.T)).to(dev).t()
+
+
+def run_device(ctx, psi, torch, dev, local_only=False):
+    m, nb = psi.shape
+    x = to_dev(psi, torch, dev)
+    y = torch.zeros((nb, m), dtype=torch.complex128, device=dev).t()
+    ctx.hk_psi(x, y, local_only=local_only)
+    torch.cuda.synchronize()
+    return y.cpu().numpy()
+
+
+def relerr(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.mark.parametrize("wname,ik,nb", [("small", 0, 3), ("small", 1, 6), ("si2", 0, 8), ("si2", 3, 5),
+                                         ("si2", 9, 1)])
+def test_device_fp64_matches_oracle(cuda, wname, ik, nb):
+    import torch
+    w = configs.WORKLOADS[wname]()
+    d = configs.kpoint_inputs(w, ik)
+    ctx = H.Context(0).setup(d)
+    psi = configs.random_psi(d["mtxd"], nb, 100 + ik)
+    got = run_device(ctx, psi, torch, cuda)
+    assert relerr(got, oracle_hpsi(d, psi, nb)) < TOL64
+
+
+def test_device_fp64_si64_box96(cuda):
+    import torch
+    w = configs.si64_cubic()
+    d = configs.kpoint_inputs(w, 0)
+    ctx = H.Context(0).setup(d)
+    psi = configs.random_psi(d["mtxd"], 6, 7)
+    got = run_device(ctx, psi, torch, cuda)
+    assert relerr(got, oracle_hpsi(d, psi, 6)) < TOL64
+
+
+def test_local_only_matches_oracle(cuda):
+    import torch
+    w = configs.si2_fcc()
+    d = configs.kpoint_inputs(w, 2)
+    ctx = H.Context(0).setup(d)
+    psi = configs.random_psi(d["mtxd"], 4, 5)
+    got = run_device(ctx, psi, torch, cuda, local_only=True)
+    ref = O.hk_psi_loc(d["mtxd"], 4, psi, d["isort"], d["vscr"], d["kmscr"], d["kgv"])
+    assert relerr(got, ref) < TOL64
+
+
+def test_band_chunking_is_invisible(cuda):
+    import torch
+    w = configs.si2_fcc()
+    d = configs.kpoint_inputs(w, 1)
+    ctx = H.Context(0).setup(d)
+    psi = configs.random_psi(d["mtxd"], 7, 9)
+    a = run_device(ctx, psi, torch, cuda)
+    ctx.set_slab_budget(1)          # one band per chunk
+    b = run_device(ctx, psi, torch, cuda)
+    assert np.array_equal(a, b)
+
+
+def test_mixed_precision_local_within_fp32_tolerance(cuda):
+    import torch
+    w = configs.si2_fcc()
+    d = configs.kpoint_inputs(w, 0)
+    ctx = H.Context(0, precision=H.MIXED).setup(d)
+    psi = configs.random_psi(d["mtxd"], 8, 3)
+    got = run_device(ctx, psi, torch, cuda)
+    assert relerr(got, oracle_hpsi(d, psi, 8)) < TOL32
+
+
+def test_dropin_host_arrays_with_leading_dimensions(cuda):
+    w = configs.small_test()
+    d = configs.kpoint_inputs(w, 1)
+    m, nb = d["mtxd"], 4
+    mxddim, mxdbnd = m + 5, nb + 2
+    psi = configs.random_psi(m, mxdbnd, 44, ld=mxddim)
+    hpsi = np.full((mxddim, mxdbnd), 7.0 + 7.0j, dtype=np.complex128, order="F")
+    anl = np.zeros((mxddim, d["nanl"] + 1), dtype=np.complex128, order="F")
+    anl[:m, : d["nanl"]] = d["anlga"]
+    xnl = np.zeros(d["nanl"] + 1)
+    xnl[: d["nanl"]] = d["xnlkb"]
+    kgv = np.asfortranarray(d["kgv"])
+    out, lnew = H.hk_psi_c16(m, nb, psi, hpsi, True, d["ng"], kgv, d["ekpg"], d["isort"], d["vscr"], d["kmscr"],
+                             anl, xnl, d["nanl"], mxddim, mxdbnd, d["nanl"] + 1, d["ng"], d["vscr"].size)
+    assert lnew is False
+    ref = oracle_hpsi(d, psi[:m], nb)
+    assert relerr(hpsi[:m, :nb], ref) < TOL64
+    assert np.all(hpsi[m:, :] == 7.0 + 7.0j) and np.all(hpsi[:, nb:] == 7.0 + 7.0j)
+    # a changed potential is picked up without any flag
+    v2 = d["vscr"] * 0.5
+    H.hk_psi_c16(m, nb, psi, hpsi, False, d["ng"], kgv, d["ekpg"], d["isort"], v2, d["kmscr"], anl, xnl,
+                 d["nanl"], mxddim, mxdbnd, d["nanl"] + 1, d["ng"], v2.size)
+    ref2 = O.hk_psi_c16(m, nb, psi[:m], d["ekpg"], d["isort"], v2, d["kmscr"], d["kgv"], d["anlga"], d["xnlkb"])
+    assert relerr(hpsi[:m, :nb], ref2) < TOL64
+    # and so is another k-point
+    d1 = configs.kpoint_inputs(w, 0)
+    m1 = d1["mtxd"]
+    psi1 = configs.random_psi(m1, nb, 45, ld=mxddim)
+    anl1 = np.zeros((mxddim, d1["nanl"]), dtype=np.complex128, order="F")
+    anl1[:m1] = d1["anlga"]
+    H.hk_psi_c16(m1, nb, psi1, hpsi, True, d1["ng"], np.asfortranarray(d1["kgv"]), d1["ekpg"], d1["isort"],
+                 d1["vscr"], d1["kmscr"], anl1, d1["xnlkb"], d1["nanl"], mxddim, mxdbnd, d1["nanl"], d1["ng"],
+                 d1["vscr"].size)
+    assert relerr(hpsi[:m1, :nb], oracle_hpsi(d1, psi1[:m1], nb)) < TOL64
+
+
+@pytest.mark.parametrize("ladd", [True, False])
+def test_dropin_nl_matches_oracle(cuda, ladd):
+    w = configs.si2_fcc()
+    d = configs.kpoint_inputs(w, 4)
+    m, nb = d["mtxd"], 3
+    psi = configs.random_psi(m, nb, 8)
+    h0 = configs.random_psi(m, nb, 9)
+    hpsi = np.asfortranarray(h0.copy())
+    H.hk_psi_nl_c16(m, nb, psi, hpsi, d["anlga"], d["xnlkb"], d["nanl"], ladd, m, nb, d["nanl"])
+    ref = O.hk_psi_nl_c16(psi, h0.copy(), d["anlga"], d["xnlkb"], ladd=ladd)
+    assert relerr(hpsi, ref) < TOL64
+
+
+def test_wraparound_box_is_rejected(cuda):
+    w = configs.small_test()
+    d = configs.kpoint_inputs(w, 0)
+    ctx = H.Context(0)
+    km = d["kmscr"].copy()
+    km[3:7] = (6, 6, 6, 6)
+    with pytest.raises(CpwB200Error) as e:
+        ctx.set_kpoint(d["mtxd"], d["isort"], d["kgv"], d["ekpg"], km)
+    assert e.value.status == 2
+
+
+def test_unsupported_box_is_rejected(cuda):
+    w = configs.small_test()
+    d = configs.kpoint_inputs(w, 0)
+    ctx = H.Context(0)
+    km = d["kmscr"].copy()
+    km[3:7] = (49, 49, 49, 49)      # 7 x 7: radix 7 is not supported
+    with pytest.raises(CpwB200Error) as e:
+        ctx.set_kpoint(d["mtxd"], d["isort"], d["kgv"], d["ekpg"], km)
+    assert e.value.status == 3
