@@ -128,7 +128,7 @@ def run_reference(args, rank):
     from oracle import c_ref
     c_ref.lib()
     nthreads = c_ref.max_threads()
-    sample = 4
+    sample = 16
     for _ in range(args.warmup):
         cpu_reference_rate(d, sample, nthreads)
     rates = []
@@ -316,16 +316,38 @@ def run_ours(args, world, rank, local, dist):
         "clocks": clocks,
     }
     if rank == 0 and world == 1:
-        rate, cores = cpu_reference_rate(d, 4)
+        rate, cores = cpu_reference_rate(d, 64, repeats=2)
         line["cpu_baseline"] = {"value": rate, "unit": "bands/s", "cores": cores, "kind": "port",
-                                "sample": "4 of 160 bands, C+OpenMP restatement of hk_psi_c16 "
+                                "sample": "64 of 160 bands, best of 2, C+OpenMP restatement of hk_psi_c16 "
                                           f"(pruned FFT + ZGEMM loops), {cores} threads"}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
 
+def run_profile(args, local):
+    """Device path only, for ncu: --bands bands of the Si64 workload, --steps+--warmup calls."""
+    import torch
+
+    from cpw2000_b200 import hk_psi as H
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    d = configs.kpoint_inputs(configs.si64_cubic(), 0)
+    nb = args.bands
+    psi = torch.from_numpy(np.ascontiguousarray(configs.random_psi(d["mtxd"], nb, 5).T)).to(dev).t()
+    hpsi = torch.empty((nb, d["mtxd"]), dtype=torch.complex128, device=dev).t()
+    ctx = H.Context(local, precision=H.MIXED if args.precision == "mixed" else H.FP64).setup(d)
+    ctx.set_slab_budget(4 << 30)
+    for _ in range(args.warmup + args.steps):
+        ctx.hk_psi(psi, hpsi)
+    torch.cuda.synchronize()
+    print(json.dumps({"mode": "profile", "bands": nb, "precision": args.precision, "calls": args.warmup + args.steps}))
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--mode", choices=["bench", "profile"], default="bench")
+    ap.add_argument("--bands", type=int, default=NB, help="profile mode: bands per call")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64", help="profile mode precision")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
@@ -333,7 +355,9 @@ def main():
     args = ap.parse_args()
     world, rank, local, dist = dist_setup(args)
     try:
-        if args.impl == "reference":
+        if args.mode == "profile":
+            run_profile(args, local)
+        elif args.impl == "reference":
             run_reference(args, rank)
         else:
             run_ours(args, world, rank, local, dist)

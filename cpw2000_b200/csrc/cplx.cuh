@@ -138,6 +138,12 @@ template <int A, int B, int S, typename T> struct DFTComp {
         const int m = (n2 * k1) % R;
         if (m == 0) {
           t[k1 * B + n2] = u[k1];
+        } else if (4 * m == R) {                 // W = i*S
+          t[k1 * B + n2] = mul_iS<S, T>(u[k1]);
+        } else if (2 * m == R) {                 // W = -1
+          t[k1 * B + n2] = mk<T>(-u[k1].x, -u[k1].y);
+        } else if (4 * m == 3 * R) {             // W = -i*S
+          t[k1 * B + n2] = mul_iS<-S, T>(u[k1]);
         } else {
           C2<T> w = mk<T>(T(tw.c[m]), T(S * tw.s[m]));
           t[k1 * B + n2] = cmul<T>(u[k1], w);
@@ -169,7 +175,8 @@ __host__ __device__ constexpr bool radix_ok(int r) {
          r == 10 || r == 12 || r == 16;
 }
 
-// Runtime radix dispatch: f(IC<R>{}) for the warp-uniform radix r.
+// Radix dispatch: with RC > 0 the radix is the compile-time RC, otherwise the
+// warp-uniform runtime r selects the instantiation: f(IC<R>{}).
 template <int N> struct IC { static constexpr int value = N; };
 template <typename F> __device__ __forceinline__ void radix_dispatch(int r, F&& f) {
   switch (r) {
@@ -185,6 +192,13 @@ template <typename F> __device__ __forceinline__ void radix_dispatch(int r, F&& 
     case 12: f(IC<12>{}); break;
     case 16: f(IC<16>{}); break;
     default: break;
+  }
+}
+template <int RC, typename F> __device__ __forceinline__ void with_radix(int r, F&& f) {
+  if constexpr (RC > 0) {
+    f(IC<RC>{});
+  } else {
+    radix_dispatch(r, static_cast<F&&>(f));
   }
 }
 

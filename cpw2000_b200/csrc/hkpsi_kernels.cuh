@@ -1,0 +1,378 @@
+// Kernel templates A, B, C of the local H|psi> (design in hkpsi_local.cuh).
+//
+// Template parameters fix the radix pair of each dimension (RX1*RX2 = n1,
+// RY1*RY2 = n2, RZ1*RZ2 = n3) and the column batch widths TC (A/C) and CB
+// (B) at compile time; 0 means "taken from the LocalPlan at run time". The
+// compile-time forms get constant index arithmetic and register allocation
+// sized for their own radices; the all-zero form serves any supported box.
+#pragma once
+#include "hkpsi_local.cuh"
+
+namespace cpwb {
+namespace kern {
+
+constexpr int kThreadsPlanes = 256;
+constexpr int kThreadsCols = 256;
+
+template <typename T> __device__ __forceinline__ C2<T> czero() { return mk<T>(T(0), T(0)); }
+
+// ---------------------------------------------------------------------------
+// A: scatter + inverse x + inverse y, one CTA per (band, kept z-plane)
+// ---------------------------------------------------------------------------
+template <typename T, int RX1, int RX2, int RY1, int RY2, int TC>
+__global__ void __launch_bounds__(kThreadsPlanes, 1)
+k_inv_xy(LocalPlan p, int band0, const C2<double>* __restrict__ psi, long long ldpsi,
+         const int* __restrict__ plane_start, const int* __restrict__ pw_idx,
+         const int* __restrict__ pw_pos, const C2<T>* __restrict__ twx,
+         const C2<T>* __restrict__ twy, C2<T>* __restrict__ W) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int tc = TC ? TC : p.tcol;
+  const int r1x = RX1 ? RX1 : p.dx.r1, r2x = RX2 ? RX2 : p.dx.r2;
+  const int r1y = RY1 ? RY1 : p.dy.r1, r2y = RY2 ? RY2 : p.dy.r2;
+  const int n1 = RX1 ? RX1 * RX2 : p.n1, n2 = RY1 ? RY1 * RY2 : p.n2;
+  const int ny = p.ny, rowp = p.rowp;
+  C2<T>* R = reinterpret_cast<C2<T>*>(smem_raw);
+  C2<T>* Tb = R + (size_t)ny * rowp;
+  C2<T>* sx = Tb + (size_t)n2 * tc;
+  C2<T>* sy = sx + n1;
+  const int zi = blockIdx.x, b = blockIdx.y;
+  const int tid = threadIdx.x, nt = blockDim.x;
+
+  for (int i = tid; i < n1; i += nt) sx[i] = twx[i];
+  for (int i = tid; i < n2; i += nt) sy[i] = twy[i];
+  for (int i = tid; i < ny * rowp; i += nt) R[i] = czero<T>();
+  __syncthreads();
+
+  const C2<double>* ps = psi + (size_t)(band0 + b) * ldpsi;
+  const int e0 = plane_start[zi], e1 = plane_start[zi + 1];
+  for (int e = e0 + tid; e < e1; e += nt) {
+    const int pos = pw_pos[e];
+    const C2<double> v = ps[pw_idx[e]];
+    R[(pos >> 16) * rowp + (pos & 0xffff)] = mk<T>(T(v.x), T(v.y));
+  }
+  __syncthreads();
+
+  // inverse x, pass 1: lines (row, n2) with the row index fastest across lanes
+  for (int it = tid; it < ny * r2x; it += nt) {
+    const int row = it % ny, n2i = it / ny;
+    C2<T>* line = R + (size_t)row * rowp + n2i;
+    with_radix<RX1>(r1x, [&](auto rc_) {
+      constexpr int RR = decltype(rc_)::value;
+      C2<T> v[RR];
+#pragma unroll
+      for (int a = 0; a < RR; ++a) v[a] = line[r2x * a];
+      DFT<RR, +1, T>::run(v);
+#pragma unroll
+      for (int a = 0; a < RR; ++a) line[r2x * a] = a == 0 ? v[0] : cmulc<T>(v[a], sx[n2i * a]);
+    });
+  }
+  __syncthreads();
+  // inverse x, pass 2: lines (row, k1), contiguous block of r2x, permuted in place
+  for (int it = tid; it < ny * r1x; it += nt) {
+    const int row = it % ny, k1 = it / ny;
+    C2<T>* line = R + (size_t)row * rowp + r2x * k1;
+    with_radix<RX2>(r2x, [&](auto rc_) {
+      constexpr int RR = decltype(rc_)::value;
+      C2<T> v[RR];
+#pragma unroll
+      for (int a = 0; a < RR; ++a) v[a] = line[a];
+      DFT<RR, +1, T>::run(v);
+#pragma unroll
+      for (int a = 0; a < RR; ++a) line[a] = v[a];
+    });
+  }
+  __syncthreads();
+
+  // inverse y on every column, in batches of tc storage positions
+  C2<T>* Wp = W + ((size_t)b * p.nz + zi) * (size_t)p.plane;
+  for (int pb = 0; pb < n1; pb += tc) {
+    const int ncol = min(tc, n1 - pb);
+    for (int it = tid; it < tc * r2y; it += nt) {
+      const int pl = it % tc, n2i = it / tc;
+      if (pl < ncol) {
+        with_radix<RY1>(r1y, [&](auto rc_) {
+          constexpr int RR = decltype(rc_)::value;
+          C2<T> v[RR];
+#pragma unroll
+          for (int a = 0; a < RR; ++a) {
+            const int y = r2y * a + n2i;
+            const int yi = idx_to_kept(y, p.kd2, n2, ny);
+            v[a] = yi >= 0 ? R[(size_t)yi * rowp + pb + pl] : czero<T>();
+          }
+          DFT<RR, +1, T>::run(v);
+#pragma unroll
+          for (int a = 0; a < RR; ++a)
+            Tb[(size_t)(r2y * a + n2i) * tc + pl] = a == 0 ? v[0] : cmulc<T>(v[a], sy[n2i * a]);
+        });
+      }
+    }
+    __syncthreads();
+    for (int it = tid; it < tc * r1y; it += nt) {
+      const int pl = it % tc, k1 = it / tc;
+      if (pl < ncol) {
+        const int pp = pb + pl;
+        const int xk1 = pp / r2x, xk2 = pp - xk1 * r2x;
+        const int x = xk1 + r1x * xk2;
+        with_radix<RY2>(r2y, [&](auto rc_) {
+          constexpr int RR = decltype(rc_)::value;
+          C2<T> v[RR];
+#pragma unroll
+          for (int a = 0; a < RR; ++a) v[a] = Tb[(size_t)(r2y * k1 + a) * tc + pl];
+          DFT<RR, +1, T>::run(v);
+#pragma unroll
+          for (int a = 0; a < RR; ++a) Wp[(size_t)(k1 + r1y * a) * n1 + x] = v[a];
+        });
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// B: inverse z, V(r)/N, forward z, one CTA per (band, CB xy-columns)
+// ---------------------------------------------------------------------------
+template <typename T, int RZ1, int RZ2, int CB>
+__global__ void __launch_bounds__(kThreadsCols, 1)
+k_z_vloc(LocalPlan p, const T* __restrict__ vr, const C2<T>* __restrict__ twz, C2<T>* __restrict__ W) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int cb = CB ? CB : p.cb;
+  const int r1 = RZ1 ? RZ1 : p.dz.r1, r2 = RZ2 ? RZ2 : p.dz.r2;
+  const int n3 = RZ1 ? RZ1 * RZ2 : p.n3;
+  C2<T>* Cs = reinterpret_cast<C2<T>*>(smem_raw);
+  C2<T>* sz = Cs + (size_t)n3 * cb;
+  const long long c0 = (long long)blockIdx.x * cb;
+  const int b = blockIdx.y;
+  const int ncol = (int)min((long long)cb, p.plane - c0);
+  const int tid = threadIdx.x, nt = blockDim.x;
+  C2<T>* Wb = W + (size_t)b * p.nz * (size_t)p.plane + c0;
+
+  for (int i = tid; i < n3; i += nt) sz[i] = twz[i];
+  for (int it = tid; it < cb * p.nz; it += nt) {
+    const int cl = it % cb, zi = it / cb;
+    if (cl < ncol) Cs[(size_t)kept_to_idx(zi, p.kd3, n3, p.nz) * cb + cl] = Wb[(size_t)zi * p.plane + cl];
+  }
+  __syncthreads();
+  // inverse pass 1 (reads only kept planes; the others are zero)
+  for (int it = tid; it < cb * r2; it += nt) {
+    const int cl = it % cb, n2i = it / cb;
+    if (cl < ncol) {
+      with_radix<RZ1>(r1, [&](auto rc_) {
+        constexpr int RR = decltype(rc_)::value;
+        C2<T> v[RR];
+#pragma unroll
+        for (int a = 0; a < RR; ++a) {
+          const int z = r2 * a + n2i;
+          v[a] = idx_to_kept(z, p.kd3, n3, p.nz) >= 0 ? Cs[(size_t)z * cb + cl] : czero<T>();
+        }
+        DFT<RR, +1, T>::run(v);
+#pragma unroll
+        for (int a = 0; a < RR; ++a)
+          Cs[(size_t)(r2 * a + n2i) * cb + cl] = a == 0 ? v[0] : cmulc<T>(v[a], sz[n2i * a]);
+      });
+    }
+  }
+  __syncthreads();
+  // inverse pass 2 -> multiply V(r)/N -> forward pass 1, in registers
+  for (int it = tid; it < cb * r1; it += nt) {
+    const int cl = it % cb, k1 = it / cb;
+    if (cl < ncol) {
+      with_radix<RZ2>(r2, [&](auto rc_) {
+        constexpr int RR = decltype(rc_)::value;
+        C2<T> v[RR];
+        T vz[RR];
+#pragma unroll
+        for (int a = 0; a < RR; ++a) vz[a] = vr[(size_t)(k1 + r1 * a) * p.plane + c0 + cl];
+#pragma unroll
+        for (int a = 0; a < RR; ++a) v[a] = Cs[(size_t)(r2 * k1 + a) * cb + cl];
+        DFT<RR, +1, T>::run(v);
+#pragma unroll
+        for (int a = 0; a < RR; ++a) v[a] = scal<T>(v[a], vz[a]);
+        DFT<RR, -1, T>::run(v);
+#pragma unroll
+        for (int a = 0; a < RR; ++a)
+          Cs[(size_t)(r2 * k1 + a) * cb + cl] = a == 0 ? v[0] : cmul<T>(v[a], sz[k1 * a]);
+      });
+    }
+  }
+  __syncthreads();
+  // forward pass 2, keep the kept planes
+  for (int it = tid; it < cb * r2; it += nt) {
+    const int cl = it % cb, m2 = it / cb;
+    if (cl < ncol) {
+      with_radix<RZ1>(r1, [&](auto rc_) {
+        constexpr int RR = decltype(rc_)::value;
+        C2<T> v[RR];
+#pragma unroll
+        for (int a = 0; a < RR; ++a) v[a] = Cs[(size_t)(r2 * a + m2) * cb + cl];
+        DFT<RR, -1, T>::run(v);
+#pragma unroll
+        for (int a = 0; a < RR; ++a) {
+          const int zi = idx_to_kept(m2 + r2 * a, p.kd3, n3, p.nz);
+          if (zi >= 0) Wb[(size_t)zi * p.plane + cl] = v[a];
+        }
+      });
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// C: forward y + forward x + gather + kinetic, one CTA per (band, kept z-plane)
+// ---------------------------------------------------------------------------
+template <typename T, int RX1, int RX2, int RY1, int RY2, int TC>
+__global__ void __launch_bounds__(kThreadsPlanes, 1)
+k_fwd_xy(LocalPlan p, int band0, const C2<double>* __restrict__ psi, long long ldpsi,
+         C2<double>* __restrict__ hpsi, long long ldh, const int* __restrict__ plane_start,
+         const int* __restrict__ pw_idx, const int* __restrict__ pw_pos,
+         const double* __restrict__ ekpg, const C2<T>* __restrict__ twx,
+         const C2<T>* __restrict__ twy, const C2<T>* __restrict__ W) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int tc = TC ? TC : p.tcol;
+  const int r1x = RX1 ? RX1 : p.dx.r1, r2x = RX2 ? RX2 : p.dx.r2;
+  const int r1y = RY1 ? RY1 : p.dy.r1, r2y = RY2 ? RY2 : p.dy.r2;
+  const int n1 = RX1 ? RX1 * RX2 : p.n1, n2 = RY1 ? RY1 * RY2 : p.n2;
+  const int ny = p.ny, rowp = p.rowp;
+  C2<T>* R = reinterpret_cast<C2<T>*>(smem_raw);
+  C2<T>* Tb = R + (size_t)ny * rowp;
+  C2<T>* sx = Tb + (size_t)n2 * tc;
+  C2<T>* sy = sx + n1;
+  const int zi = blockIdx.x, b = blockIdx.y;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int i = tid; i < n1; i += nt) sx[i] = twx[i];
+  for (int i = tid; i < n2; i += nt) sy[i] = twy[i];
+
+  const C2<T>* Wp = W + ((size_t)b * p.nz + zi) * (size_t)p.plane;
+  for (int xb = 0; xb < n1; xb += tc) {
+    const int ncol = min(tc, n1 - xb);
+    for (int it = tid; it < tc * n2; it += nt) {
+      const int xl = it % tc, y = it / tc;
+      if (xl < ncol) Tb[(size_t)y * tc + xl] = Wp[(size_t)y * n1 + xb + xl];
+    }
+    __syncthreads();
+    for (int it = tid; it < tc * r2y; it += nt) {
+      const int xl = it % tc, n2i = it / tc;
+      if (xl < ncol) {
+        with_radix<RY1>(r1y, [&](auto rc_) {
+          constexpr int RR = decltype(rc_)::value;
+          C2<T> v[RR];
+#pragma unroll
+          for (int a = 0; a < RR; ++a) v[a] = Tb[(size_t)(r2y * a + n2i) * tc + xl];
+          DFT<RR, -1, T>::run(v);
+#pragma unroll
+          for (int a = 0; a < RR; ++a)
+            Tb[(size_t)(r2y * a + n2i) * tc + xl] = a == 0 ? v[0] : cmul<T>(v[a], sy[n2i * a]);
+        });
+      }
+    }
+    __syncthreads();
+    for (int it = tid; it < tc * r1y; it += nt) {
+      const int xl = it % tc, k1 = it / tc;
+      if (xl < ncol) {
+        with_radix<RY2>(r2y, [&](auto rc_) {
+          constexpr int RR = decltype(rc_)::value;
+          C2<T> v[RR];
+#pragma unroll
+          for (int a = 0; a < RR; ++a) v[a] = Tb[(size_t)(r2y * k1 + a) * tc + xl];
+          DFT<RR, -1, T>::run(v);
+#pragma unroll
+          for (int a = 0; a < RR; ++a) {
+            const int yi = idx_to_kept(k1 + r1y * a, p.kd2, n2, ny);
+            if (yi >= 0) R[(size_t)yi * rowp + xb + xl] = v[a];
+          }
+        });
+      }
+    }
+    __syncthreads();
+  }
+
+  // forward x on the kept rows (row index fastest across lanes)
+  for (int it = tid; it < ny * r2x; it += nt) {
+    const int row = it % ny, n2i = it / ny;
+    C2<T>* line = R + (size_t)row * rowp + n2i;
+    with_radix<RX1>(r1x, [&](auto rc_) {
+      constexpr int RR = decltype(rc_)::value;
+      C2<T> v[RR];
+#pragma unroll
+      for (int a = 0; a < RR; ++a) v[a] = line[r2x * a];
+      DFT<RR, -1, T>::run(v);
+#pragma unroll
+      for (int a = 0; a < RR; ++a) line[r2x * a] = a == 0 ? v[0] : cmul<T>(v[a], sx[n2i * a]);
+    });
+  }
+  __syncthreads();
+  for (int it = tid; it < ny * r1x; it += nt) {
+    const int row = it % ny, k1 = it / ny;
+    C2<T>* line = R + (size_t)row * rowp + r2x * k1;
+    with_radix<RX2>(r2x, [&](auto rc_) {
+      constexpr int RR = decltype(rc_)::value;
+      C2<T> v[RR];
+#pragma unroll
+      for (int a = 0; a < RR; ++a) v[a] = line[a];
+      DFT<RR, -1, T>::run(v);
+#pragma unroll
+      for (int a = 0; a < RR; ++a) line[a] = v[a];
+    });
+  }
+  __syncthreads();
+
+  // gather the sphere (permuted x storage) and add the kinetic diagonal
+  const C2<double>* ps = psi + (size_t)(band0 + b) * ldpsi;
+  C2<double>* hp = hpsi + (size_t)(band0 + b) * ldh;
+  const int e0 = plane_start[zi], e1 = plane_start[zi + 1];
+  for (int e = e0 + tid; e < e1; e += nt) {
+    const int pos = pw_pos[e];
+    const int x = pos & 0xffff, yi = pos >> 16;
+    const int q = x / r1x;
+    const int pp = r2x * (x - q * r1x) + q;
+    const C2<T> v = R[(size_t)yi * rowp + pp];
+    const int i = pw_idx[e];
+    C2<double> out = mk<double>(double(v.x), double(v.y));
+    if (ekpg) {
+      const C2<double> s = ps[i];
+      const double ek = ekpg[i];
+      out.x += ek * s.x;
+      out.y += ek * s.y;
+    }
+    hp[i] = out;
+  }
+}
+
+// Launch A, B, C for one band chunk with one compile-time configuration.
+template <typename T, int RX1, int RX2, int RY1, int RY2, int RZ1, int RZ2, int TC, int CB>
+cudaError_t launch_impl(const LocalPlan& p, int nbc, int band0, const C2<double>* psi, long long ldpsi,
+                        C2<double>* hpsi, long long ldh, const int* plane_start, const int* pw_idx,
+                        const int* pw_pos, const double* ekpg, const T* vr, const C2<T>* twx, const C2<T>* twy,
+                        const C2<T>* twz, C2<T>* W, cudaStream_t st, cudaEvent_t* ev) {
+  const size_t sm_pl = smem_planes<T>(p);
+  const size_t sm_co = smem_columns<T>(p);
+  auto* ka = k_inv_xy<T, RX1, RX2, RY1, RY2, TC>;
+  auto* kb = k_z_vloc<T, RZ1, RZ2, CB>;
+  auto* kc = k_fwd_xy<T, RX1, RX2, RY1, RY2, TC>;
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pl)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pl)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_co)) != cudaSuccess) return e;
+  dim3 gA(p.nz, nbc);
+  if (ev) cudaEventRecord(ev[0], st);
+  ka<<<gA, kThreadsPlanes, sm_pl, st>>>(p, band0, psi, ldpsi, plane_start, pw_idx, pw_pos, twx, twy, W);
+  if (ev) cudaEventRecord(ev[1], st);
+  dim3 gB((unsigned)((p.plane + p.cb - 1) / p.cb), nbc);
+  kb<<<gB, kThreadsCols, sm_co, st>>>(p, vr, twz, W);
+  if (ev) cudaEventRecord(ev[2], st);
+  kc<<<gA, kThreadsPlanes, sm_pl, st>>>(p, band0, psi, ldpsi, hpsi, ldh, plane_start, pw_idx, pw_pos, ekpg, twx,
+                                        twy, W);
+  if (ev) cudaEventRecord(ev[3], st);
+  return cudaGetLastError();
+}
+
+}  // namespace kern
+
+#define CPWB_LAUNCH_ARGS(T)                                                                                  \
+  const LocalPlan &p, int nbc, int band0, const C2<double>*psi, long long ldpsi, C2<double>*hpsi,            \
+      long long ldh, const int *plane_start, const int *pw_idx, const int *pw_pos, const double *ekpg,       \
+      const T *vr, const C2<T>*twx, const C2<T>*twy, const C2<T>*twz, C2<T>*W, cudaStream_t st,             \
+      cudaEvent_t *ev
+
+#define CPWB_INSTANTIATE(T, RX1, RX2, RY1, RY2, RZ1, RZ2, TC, CB) \
+  template cudaError_t kern::launch_impl<T, RX1, RX2, RY1, RY2, RZ1, RZ2, TC, CB>(CPWB_LAUNCH_ARGS(T));
+
+}  // namespace cpwb

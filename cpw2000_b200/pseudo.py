@@ -200,8 +200,14 @@ def local_potential_box(species, adot, box, idpad: int = 0):
     vg = np.zeros(mm.shape[1], dtype=np.complex128)
     for sp in species:
         ff = -sp.v0 * (2 * PI * sp.sigma ** 2) ** 1.5 * np.exp(-0.5 * g2 * sp.sigma ** 2) / vcell
-        phase = np.exp(-2j * PI * (sp.rat @ mm)).sum(axis=0)
-        vg += ff * phase
+        # structure factor sum_a e^{-2 pi i m.rat_a}, separable in the three directions
+        p1 = np.exp(-2j * PI * np.outer(sp.rat[:, 0], m[0]))          # (natom, n1)
+        p2 = np.exp(-2j * PI * np.outer(sp.rat[:, 1], m[1]))
+        p3 = np.exp(-2j * PI * np.outer(sp.rat[:, 2], m[2]))
+        sf = np.empty((n1, n2, n3), dtype=np.complex128)
+        for k in range(n3):
+            sf[:, :, k] = (p1 * p3[:, k:k + 1]).T @ p2
+        vg += ff * sf.reshape(-1)
     vg = vg.reshape(n1, n2, n3)
     for ax, n in enumerate((n1, n2, n3)):
         if n % 2 == 0:

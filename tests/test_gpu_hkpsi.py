@@ -63,6 +63,28 @@ def test_device_fp64_si64_box96(cuda):
     assert relerr(got, oracle_hpsi(d, psi, 6)) < TOL64
 
 
+@pytest.mark.parametrize("prec,tol", [(0, TOL64), (1, TOL32)])
+def test_device_box40_kpoint_batch_cell(cuda, prec, tol):
+    import torch
+    w = configs.si8_cubic_kbatch()
+    d = configs.kpoint_inputs(w, 3)
+    ctx = H.Context(0, precision=prec).setup(d)
+    psi = configs.random_psi(d["mtxd"], 5, 13)
+    got = run_device(ctx, psi, torch, cuda)
+    assert relerr(got, oracle_hpsi(d, psi, 5)) < tol
+
+
+@pytest.mark.parametrize("prec,tol", [(0, TOL64), (1, TOL32)])
+def test_device_box144_si216(cuda, prec, tol):
+    import torch
+    w = configs.si216_cubic()
+    d = configs.kpoint_inputs(w, 1)
+    ctx = H.Context(0, precision=prec).setup(d)
+    psi = configs.random_psi(d["mtxd"], 2, 17)
+    got = run_device(ctx, psi, torch, cuda)
+    assert relerr(got, oracle_hpsi(d, psi, 2)) < tol
+
+
 def test_local_only_matches_oracle(cuda):
     import torch
     w = configs.si2_fcc()
