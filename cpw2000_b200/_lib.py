@@ -41,6 +41,7 @@ SIGNATURES = {
     "hk_psi_c16_": (None, [IP, IP, DP, DP, IP, IP, IP, DP, IP, DP, IP, DP, DP, IP, IP, IP, IP, IP, IP]),
     "cpw_b200_hk_psi_nl_c16": (I, [IP, IP, DP, DP, DP, DP, IP, IP, IP, IP, IP]),
     "hk_psi_nl_c16_": (None, [IP, IP, DP, DP, DP, DP, IP, IP, IP, IP, IP]),
+    "cpw_b200_hk_psi_loc_noalloc": (I, [I, I, P, LL, P, LL, P, P, P, IP, P]),
 }
 
 

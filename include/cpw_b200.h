@@ -118,6 +118,29 @@ void hk_psi_nl_c16_(const int* mtxd, const int* neig, const double* psi, double*
                     const double* xnlkb, const int* nanl, const int* ladd, const int* mxddim, const int* mxdbnd,
                     const int* mxdanl);
 
+/* ---- allocation-free local H|psi> ----
+ * No counterpart in the reference. For callers that cannot call cudaMalloc
+ * (a caller-owned memory pool or fixed device-memory budget, a host code that
+ * owns every device buffer and forbids the library to grow the device heap,
+ * or a region where an allocation would synchronise the device):
+ * hpsi = V_loc psi (+ ekpg psi when ekpg is not NULL), the local part of
+ * hk_psi_c16, FP64, on `stream` (cudaStream_t; NULL = legacy default stream).
+ * Every pointer except kmscr is device memory owned by the caller: psi/hpsi
+ * complex128 column-major (ld >= mtxd), kgvb(3, mtxd) = kgv(:, isort(i)) of
+ * the basis, ekpg(mtxd) or NULL, vscr(id*n2*n3) in the reference layout;
+ * kmscr(7) is host memory. The call allocates nothing: its work space (FFT
+ * slab of a band chunk, plane lists, twiddles, repacked potential) is one
+ * fixed device array of CPW_B200_NOALLOC_SCRATCH_BYTES held by every GPU that
+ * loads the library until the process exits. Sizes whose set-up data or one
+ * band's FFT slab do not fit are rejected with CPW_B200_BAD_ARG and a message.
+ * All calls share the array: calls that overlap on the GPU race, so serialise
+ * them. The first call on a device looks up the array's address with that
+ * device current; make it before any stream capture. */
+#define CPW_B200_NOALLOC_SCRATCH_BYTES (64LL << 20)
+int cpw_b200_hk_psi_loc_noalloc(int mtxd, int neig, const void* psi, long long ldpsi, void* hpsi, long long ldhpsi,
+                                const int* kgvb, const double* ekpg, const double* vscr, const int* kmscr,
+                                void* stream);
+
 #ifdef __cplusplus
 }
 #endif
