@@ -77,6 +77,48 @@ int d2h_cols(double* dst, long long ldd, const void* src, long long lds, long lo
   return e == cudaSuccess ? kOk : cuda_fail(e, "cudaMemcpy2D D2H");
 }
 
+
+// Bring the default context in line with the arguments of a drop-in call: the
+// k-point arrays and vscr are compared with the previous call's shadows and
+// re-uploaded only when they changed; the projectors when lnewanl is set, the
+// basis changed or nanl changed (then lnewanl is cleared).
+int sync_dropin_inputs(cpw_b200_ctx* c, int m, int ng, const int* kgv, const double* ekpg, const int* isort,
+                       const double* vscr, const int* kmscr, const double* anlga, const double* xnlkb, int nanl,
+                       int mxddim, int mxdscr, int* lnewanl) {
+  std::vector<int> kg((size_t)3 * m);
+  for (int i = 0; i < m; ++i) {
+    const int it = isort[i];
+    if (it < 1 || it > ng) return fail(kBadArg, "isort out of range of kgv");
+    for (int j = 0; j < 3; ++j) kg[3 * (size_t)i + j] = kgv[3 * (size_t)(it - 1) + j];
+  }
+  const bool kchanged = !c->have_basis || c->sh_mtxd != m || !same(c->sh_kmscr, kmscr, 7) ||
+                        !same(c->sh_isort, isort, (size_t)m) || !same(c->sh_kgv, kg.data(), kg.size()) ||
+                        !same(c->sh_ekpg, ekpg, (size_t)m);
+  int s;
+  if (kchanged) {
+    // the compact kgv(3, mtxd) of the basis with isort = 1..mtxd is what the device needs
+    std::vector<int> iota(m);
+    for (int i = 0; i < m; ++i) iota[i] = i + 1;
+    if ((s = ctx_set_basis(c, m, iota.data(), kg.data(), m, ekpg, kmscr))) return s;
+    c->sh_mtxd = m;
+    c->sh_kmscr.assign(kmscr, kmscr + 7);
+    c->sh_isort.assign(isort, isort + m);
+    c->sh_kgv = kg;
+    c->sh_ekpg.assign(ekpg, ekpg + m);
+    c->sh_vscr.clear();
+  }
+  const size_t nv = (size_t)kmscr[6] * kmscr[4] * kmscr[5];
+  if (!c->have_pot || !same(c->sh_vscr, vscr, nv)) {
+    if ((s = ctx_set_potential(c, vscr, mxdscr))) return s;
+    c->sh_vscr.assign(vscr, vscr + nv);
+  }
+  if (kchanged || *lnewanl != 0 || c->nanl != nanl) {
+    if ((s = ctx_set_projectors(c, nanl, anlga, mxddim, xnlkb, false))) return s;
+    *lnewanl = 0;
+  }
+  return kOk;
+}
+
 [[noreturn]] void stop_like_fortran(const char* routine) {
   printf("\n   STOPPED in %s:  %s\n", routine, cpwb::last_error());
   fflush(stdout);
@@ -247,38 +289,10 @@ int cpw_b200_hk_psi_c16(const int* mtxd, const int* neig, const double* psi, dou
   if (int s = default_ctx(&c)) return s;
   cudaSetDevice(c->device);
   const int m = *mtxd, nb = *neig;
-  // k-point arrays: re-upload when any of them changed
-  std::vector<int> kg((size_t)3 * m);
-  for (int i = 0; i < m; ++i) {
-    const int it = isort[i];
-    if (it < 1 || it > *ng) return fail(kBadArg, "hk_psi_c16: isort out of range");
-    for (int j = 0; j < 3; ++j) kg[3 * (size_t)i + j] = kgv[3 * (size_t)(it - 1) + j];
-  }
-  bool kchanged = !c->have_basis || c->sh_mtxd != m || !same(c->sh_kmscr, kmscr, 7) ||
-                  !same(c->sh_isort, isort, (size_t)m) || !same(c->sh_kgv, kg.data(), kg.size()) ||
-                  !same(c->sh_ekpg, ekpg, (size_t)m);
   int s;
-  if (kchanged) {
-    // the compact kgv(3, mtxd) of the basis with isort = 1..mtxd is what the device needs
-    std::vector<int> iota(m);
-    for (int i = 0; i < m; ++i) iota[i] = i + 1;
-    if ((s = ctx_set_basis(c, m, iota.data(), kg.data(), m, ekpg, kmscr))) return s;
-    c->sh_mtxd = m;
-    c->sh_kmscr.assign(kmscr, kmscr + 7);
-    c->sh_isort.assign(isort, isort + m);
-    c->sh_kgv = kg;
-    c->sh_ekpg.assign(ekpg, ekpg + m);
-    c->sh_vscr.clear();
-  }
-  const size_t nv = (size_t)kmscr[6] * kmscr[4] * kmscr[5];
-  if (!c->have_pot || !same(c->sh_vscr, vscr, nv)) {
-    if ((s = ctx_set_potential(c, vscr, *mxdscr))) return s;
-    c->sh_vscr.assign(vscr, vscr + nv);
-  }
-  if (kchanged || *lnewanl != 0 || c->nanl != *nanl) {
-    if ((s = ctx_set_projectors(c, *nanl, anlga, *mxddim, xnlkb, false))) return s;
-    *lnewanl = 0;
-  }
+  if ((s = sync_dropin_inputs(c, m, *ng, kgv, ekpg, isort, vscr, kmscr, anlga, xnlkb, *nanl, *mxddim, *mxdscr,
+                              lnewanl)))
+    return s;
   if (m == 0 || nb == 0) return kOk;
   const size_t bytes = (size_t)m * nb * 16;
   if ((s = c->h_in.ensure(bytes))) return s;
@@ -297,6 +311,72 @@ void hk_psi_c16_(const int* mtxd, const int* neig, const double* psi, double* hp
   int s = cpw_b200_hk_psi_c16(mtxd, neig, psi, hpsi, lnewanl, ng, kgv, ekpg, isort, vscr, kmscr, anlga, xnlkb, nanl,
                               mxddim, mxdbnd, mxdanl, mxdgve, mxdscr);
   if (s) stop_like_fortran("hk_psi_c16");
+}
+
+int cpw_b200_ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, double epspsi, int* neig,
+                          int mtxds, void* psi, long long ldpsi, void* hpsi, double* ei, const double* hamsm,
+                          int mxdsml, const double* hdiag, int mxdbnd, long long* ihkpsum, void* stream) {
+  if (int s = check_ctx(c)) return s;
+  cudaSetDevice(c->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  long long ih = 0;
+  int s = ditsp_device(c, ipr, ifail, icmax, iguess, epspsi, neig, mtxds, psi, ldpsi, hpsi, hamsm, mxdsml, hdiag,
+                       mxdbnd, ei, &ih, st);
+  if (ihkpsum) *ihkpsum = ih;
+  return s;
+}
+
+int cpw_b200_ditsp_c16(const int* ipr, int* ifail, const int* icmax, const int* iguess, const double* epspsi,
+                       int* lnewanl, int* neig, const int* mtxd, const int* mtxds, double* psi, double* hpsi,
+                       double* ei, const double* ekpg, const int* isort, const double* vscr, const int* kmscr,
+                       const int* ng, const int* kgv, const double* anlga, const double* xnlkb, const int* nanl,
+                       const double* hamsm, const double* hdiag, const int* mxddim, const int* mxdsml,
+                       const int* mxdbnd, const int* mxdgve, const int* mxdscr, const int* mxdanl) {
+  // argument checks of ditsp_c16.f90:143-210
+  *ifail = 0;
+  if (*neig < 1) return kOk;
+  if (*neig > *mtxds) return fail(kBadArg, "ditsp_c16: neig is greater than mtxds");
+  if (*neig > *mxdbnd) return fail(kBadArg, "ditsp_c16: neig is greater than mxdbnd");
+  if (3 * *neig > *mxdsml) return fail(kBadArg, "ditsp_c16: 3*neig is greater than mxdsml");
+  if (*mtxds > *mxdsml) return fail(kBadArg, "ditsp_c16: mtxds is greater than mxdsml");
+  if (*mtxd > *mxddim) return fail(kBadArg, "ditsp_c16: mtxd is greater than mxddim");
+  if (*nanl > *mxdanl) return fail(kBadArg, "ditsp_c16: nanl is greater than mxdanl");
+  if (*ng > *mxdgve) return fail(kBadArg, "ditsp_c16: ng is greater than mxdgve");
+  cpw_b200_ctx* c;
+  if (int s = default_ctx(&c)) return s;
+  cudaSetDevice(c->device);
+  const int m = *mtxd, nb = *mxdbnd;
+  int s;
+  if ((s = sync_dropin_inputs(c, m, *ng, kgv, ekpg, isort, vscr, kmscr, anlga, xnlkb, *nanl, *mxddim, *mxdscr,
+                              lnewanl)))
+    return s;
+  const size_t bytes = (size_t)m * nb * 16;
+  if ((s = c->h_in.ensure(bytes))) return s;
+  if ((s = c->h_out.ensure(bytes))) return s;
+  if ((s = h2d_cols(c->h_in.p, m, psi, *mxddim, m, nb, c->stream))) return s;
+  if ((s = h2d_cols(c->h_out.p, m, hpsi, *mxddim, m, nb, c->stream))) return s;
+  long long ih = 0;
+  const int sd = ditsp_device(c, *ipr, ifail, *icmax, *iguess, *epspsi, neig, *mtxds, c->h_in.p, m, c->h_out.p, hamsm,
+                              *mxdsml, hdiag, nb, ei, &ih, c->stream);
+  if (sd != kOk && sd != kNotConverged) return sd;
+  if ((s = d2h_cols(psi, *mxddim, c->h_in.p, m, m, nb, c->stream))) return s;
+  if ((s = d2h_cols(hpsi, *mxddim, c->h_out.p, m, m, nb, c->stream))) return s;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "ditsp_c16");
+  return sd;
+}
+
+void ditsp_c16_(const int* ipr, int* ifail, const int* icmax, const int* iguess, const double* epspsi, int* lnewanl,
+                int* neig, const int* mtxd, const int* mtxds, double* psi, double* hpsi, double* ei,
+                const double* ekpg, const int* isort, const double* vscr, const int* kmscr, const int* ng,
+                const int* kgv, const double* anlga, const double* xnlkb, const int* nanl, const double* hamsm,
+                const double* hdiag, const int* mxddim, const int* mxdsml, const int* mxdbnd, const int* mxdgve,
+                const int* mxdscr, const int* mxdanl) {
+  int s = cpw_b200_ditsp_c16(ipr, ifail, icmax, iguess, epspsi, lnewanl, neig, mtxd, mtxds, psi, hpsi, ei, ekpg, isort,
+                             vscr, kmscr, ng, kgv, anlga, xnlkb, nanl, hamsm, hdiag, mxddim, mxdsml, mxdbnd, mxdgve,
+                             mxdscr, mxdanl);
+  // not converged is reported through ifail, as the reference does (ditsp_c16.f90:412)
+  if (s != 0 && s != CPW_B200_NOT_CONVERGED) stop_like_fortran("ditsp_c16");
 }
 
 int cpw_b200_hk_psi_nl_c16(const int* mtxd, const int* neig, const double* psi, double* hpsi, const double* anlga,

@@ -1,0 +1,903 @@
+// Block iterative eigensolver on the GPU, restating Src/ditsp (ditsp_c16 and
+// its start/loop/ritz parts, the block Gram-Schmidt family, diag_c16,
+// diag_rq_jac_c16 and ditsp_error). The control flow runs on the host with the
+// reference's decisions and thresholds; every vector block (psi, hpsi, the
+// iterative basis bas/hbas) stays in device memory. Dense products are cuBLAS
+// ZGEMMs, the subspace eigensolve is cuSOLVER zheevd ('V', lower), and the
+// column reductions / Jacobi relaxation are the kernels below. H|psi> is the
+// context's operator (FP64 drop-in or the mixed-precision form).
+#include <cusolverDn.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <complex>
+#include <string>
+#include <vector>
+
+#include "../../include/cpw_b200.h"
+#include "context.hpp"
+
+namespace cpwb {
+namespace {
+
+using Z = cuDoubleComplex;
+using zc = std::complex<double>;
+
+float r4(double x) { return (float)x; }
+// Fortran default-real literals as the reference compiles them
+const double C0P2 = r4(0.2), C0P01 = r4(0.01), C0P95 = r4(0.95), C0P99 = r4(0.99), C0P9999 = r4(0.9999);
+const double C1P2 = r4(1.2), CEPS20 = r4(1.0e-20);
+
+// --------------------------- column kernels ---------------------------
+constexpr int kColThreads = 256;
+
+// Sum over the block, returned to every thread (fixed order: deterministic).
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = lane < (blockDim.x >> 5) ? sh[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[32] = v;
+  }
+  __syncthreads();
+  v = sh[32];
+  __syncthreads();
+  return v;
+}
+
+// out[j] = sum_i conj(x_ij) y_ij, one CTA per column (deterministic order)
+__global__ void k_coldot(int m, const Z* __restrict__ x, long long ldx, const Z* __restrict__ y, long long ldy,
+                         Z* __restrict__ out) {
+  __shared__ double sh[33];
+  const int j = blockIdx.x;
+  const Z* a = x + (size_t)j * ldx;
+  const Z* b = y + (size_t)j * ldy;
+  double re = 0, im = 0;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    const Z u = a[i], v = b[i];
+    re += u.x * v.x + u.y * v.y;
+    im += u.x * v.y - u.y * v.x;
+  }
+  re = block_sum(re, sh);
+  im = block_sum(im, sh);
+  if (threadIdx.x == 0) out[j] = make_cuDoubleComplex(re, im);
+}
+
+// eg[j] = Re<p_j|h_j>; res[j] = || h_j - eg_j p_j ||^2 (two passes, no cancellation)
+__global__ void k_rayleigh_residual(int m, const Z* __restrict__ p, long long ldp, const Z* __restrict__ h,
+                                    long long ldh, double* __restrict__ eg, double* __restrict__ res) {
+  __shared__ double sh[33];
+  const int j = blockIdx.x;
+  const Z* a = p + (size_t)j * ldp;
+  const Z* b = h + (size_t)j * ldh;
+  double re = 0;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) re += a[i].x * b[i].x + a[i].y * b[i].y;
+  const double e = block_sum(re, sh);
+  double r = 0;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    const double dx = b[i].x - e * a[i].x, dy = b[i].y - e * a[i].y;
+    r += dx * dx + dy * dy;
+  }
+  r = block_sum(r, sh);
+  if (threadIdx.x == 0) {
+    eg[j] = e;
+    res[j] = r;
+  }
+}
+
+// relaxation step (ditsp_c16_loop.f90:531-543 with diag_rq_jac_c16.f90:67-79):
+// r = h - eg p; x = hdiag - eg; x = 1 if x < 1 else 1/x; p += -x r
+__global__ void k_jacobi(int m, Z* __restrict__ p, long long ldp, const Z* __restrict__ h, long long ldh,
+                         const double* __restrict__ eg, const double* __restrict__ hdiag) {
+  const int j = blockIdx.y;
+  const double e = eg[j];
+  Z* a = p + (size_t)j * ldp;
+  const Z* b = h + (size_t)j * ldh;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    double x = hdiag[i] - e;
+    x = x < 1.0 ? 1.0 : 1.0 / x;
+    const Z u = a[i], v = b[i];
+    a[i] = make_cuDoubleComplex(u.x - x * (v.x - e * u.x), u.y - x * (v.y - e * u.y));
+  }
+}
+
+// x_j *= s_j (real)
+__global__ void k_colscale(int m, Z* __restrict__ x, long long ldx, const double* __restrict__ s) {
+  const int j = blockIdx.y;
+  const double f = s[j];
+  Z* a = x + (size_t)j * ldx;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+    a[i] = make_cuDoubleComplex(a[i].x * f, a[i].y * f);
+}
+
+// y_j -= c_j x_j  (complex c on device)
+__global__ void k_colaxpy(int m, const Z* __restrict__ x, long long ldx, Z* __restrict__ y, long long ldy,
+                          const Z* __restrict__ c) {
+  const int j = blockIdx.y;
+  const Z f = c[j];
+  const Z* a = x + (size_t)j * ldx;
+  Z* b = y + (size_t)j * ldy;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    const Z u = a[i];
+    b[i] = make_cuDoubleComplex(b[i].x - (f.x * u.x - f.y * u.y), b[i].y - (f.x * u.y + f.y * u.x));
+  }
+}
+
+// --------------------------- solver state ---------------------------
+struct Solver {
+  cpw_b200_ctx* c;
+  cudaStream_t st;
+  cublasHandle_t blas;
+  cusolverDnHandle_t sol = nullptr;
+  int m;            // mtxd
+  int mxdsml, mxdbnd;
+  long long ldp;    // leading dim of psi/hpsi (device)
+  Z* P;             // psi   (ldp x mxdbnd)
+  Z* HP;            // hpsi
+  DevBuf bas, hbas, smallA, smallV, dvec, dvec2, dz, work, info, eg_d, hdiag_d;
+  int lwork = 0;
+  long long ihk = 0;
+  int status = kOk;
+  const Z one = make_cuDoubleComplex(1, 0), zero = make_cuDoubleComplex(0, 0), mone = make_cuDoubleComplex(-1, 0);
+
+  Z* B(int j) { return (Z*)bas.p + (size_t)j * m; }
+  Z* HB(int j) { return (Z*)hbas.p + (size_t)j * m; }
+  Z* Pc(int j) { return P + (size_t)j * ldp; }
+  Z* HPc(int j) { return HP + (size_t)j * ldp; }
+
+  int ck(cudaError_t e, const char* w) { return e == cudaSuccess ? kOk : cuda_fail(e, w); }
+  int ckb(cublasStatus_t s, const char* w) {
+    return s == CUBLAS_STATUS_SUCCESS ? kOk : fail(kCublas, std::string(w) + ": cuBLAS status " + std::to_string((int)s));
+  }
+
+  int hk(Z* x, long long ldx, Z* hx, long long ldhx, int n) {
+    if (n <= 0) return kOk;
+    ihk += n;
+    return ctx_hkpsi_device(c, n, x, ldx, hx, ldhx, st, true, true);
+  }
+
+  // C(m x n) = alpha * op(A) * op(B) + beta * C
+  int gemm(cublasOperation_t ta, cublasOperation_t tb, int mm, int nn, int kk, Z alpha, const Z* A, long long lda,
+           const Z* Bm, long long ldb, Z beta, Z* Cm, long long ldc, const char* w) {
+    if (mm <= 0 || nn <= 0) return kOk;
+    if (kk <= 0) {
+      // C = beta C
+      if (beta.x == 0 && beta.y == 0) {
+        for (int j = 0; j < nn; ++j)
+          if (int s = ck(cudaMemsetAsync(Cm + (size_t)j * ldc, 0, sizeof(Z) * mm, st), w)) return s;
+      }
+      return kOk;
+    }
+    return ckb(cublasZgemm(blas, ta, tb, mm, nn, kk, &alpha, A, (int)lda, Bm, (int)ldb, &beta, Cm, (int)ldc), w);
+  }
+
+  // host copies of per-column dots  out[j] = <x_j|y_j>
+  int coldots(const Z* x, long long ldx, const Z* y, long long ldy, int n, std::vector<zc>& out) {
+    out.assign(n, zc(0, 0));
+    if (n <= 0) return kOk;
+    if (int s = dz.ensure(sizeof(Z) * n)) return s;
+    k_coldot<<<n, kColThreads, 0, st>>>(m, x, ldx, y, ldy, (Z*)dz.p);
+    if (int s = ck(cudaMemcpyAsync(out.data(), dz.p, sizeof(Z) * n, cudaMemcpyDeviceToHost, st), "coldots")) return s;
+    return ck(cudaStreamSynchronize(st), "coldots");
+  }
+
+  int colscale(Z* x, long long ldx, int n, const std::vector<double>& s) {
+    if (n <= 0) return kOk;
+    if (int r = dvec2.ensure(sizeof(double) * n)) return r;
+    if (int r = ck(cudaMemcpyAsync(dvec2.p, s.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st), "colscale"))
+      return r;
+    dim3 g((unsigned)std::min(64, (m + 255) / 256), n);
+    k_colscale<<<g, 256, 0, st>>>(m, x, ldx, (const double*)dvec2.p);
+    // the host vector may go out of scope: wait for the copy
+    return ck(cudaStreamSynchronize(st), "colscale");
+  }
+
+  // y -= c x for single columns (c host value)
+  int axpy1(const Z* x, Z* y, zc cf) {
+    if (int s = dz.ensure(sizeof(Z) * 8)) return s;
+    Z v = make_cuDoubleComplex(cf.real(), cf.imag());
+    if (int s = ck(cudaMemcpyAsync(dz.p, &v, sizeof(Z), cudaMemcpyHostToDevice, st), "axpy")) return s;
+    dim3 g((unsigned)std::min(64, (m + 255) / 256), 1);
+    k_colaxpy<<<g, 256, 0, st>>>(m, x, m, y, m, (const Z*)dz.p);
+    return ck(cudaStreamSynchronize(st), "axpy");
+  }
+
+  int copycols(Z* dst, long long ldd, const Z* src, long long lds, int n) {
+    if (n <= 0) return kOk;
+    return ck(cudaMemcpy2DAsync(dst, ldd * sizeof(Z), src, lds * sizeof(Z), m * sizeof(Z), n,
+                                cudaMemcpyDeviceToDevice, st),
+              "copycols");
+  }
+
+  // Hermitian eigen-decomposition of the n x n device matrix A (ld n) with
+  // zheevd('V','L'): eigenvalues to host w, eigenvectors overwrite A.
+  int diag(Z* A, int n, std::vector<double>& w) {
+    w.assign(n, 0.0);
+    if (n <= 0) return kOk;
+    if (!sol) {
+      if (cusolverDnCreate(&sol) != CUSOLVER_STATUS_SUCCESS) return fail(kCusolver, "cusolverDnCreate failed");
+    }
+    cusolverDnSetStream(sol, st);
+    int lw = 0;
+    if (cusolverDnZheevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, A, n,
+                                    (double*)eg_d.p, &lw) != CUSOLVER_STATUS_SUCCESS)
+      return fail(kCusolver, "zheevd buffer size");
+    if (int s = work.ensure(sizeof(Z) * (size_t)std::max(lw, 1))) return s;
+    if (int s = info.ensure(sizeof(int))) return s;
+    if (cusolverDnZheevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, A, n, (double*)eg_d.p,
+                         (Z*)work.p, lw, (int*)info.p) != CUSOLVER_STATUS_SUCCESS)
+      return fail(kCusolver, "zheevd");
+    int inf = 0;
+    if (int s = ck(cudaMemcpyAsync(&inf, info.p, sizeof(int), cudaMemcpyDeviceToHost, st), "zheevd info")) return s;
+    if (int s = ck(cudaMemcpyAsync(w.data(), eg_d.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st), "zheevd w"))
+      return s;
+    if (int s = ck(cudaStreamSynchronize(st), "zheevd")) return s;
+    if (inf != 0) return fail(kCusolver, "diag_c16 failed, info = " + std::to_string(inf));
+    return kOk;
+  }
+
+  // ---- block Gram-Schmidt family (grsch_mod / grsch_mm / grsch_loop / grsch_shift) ----
+  int grsch_mod(bool also, Z* x, Z* hx, int nvec, int* irow, const double* xscl) {
+    const double eps = CEPS20;
+    const double peq = (1.0 / eps) * 2.2250738585072014e-308;
+    std::vector<zc> d;
+    for (int i = 0; i < nvec; ++i) {
+      Z* xi = x + (size_t)i * m;
+      Z* hxi = also ? hx + (size_t)i * m : nullptr;
+      if (i > 0) {
+        if (int s = coldots(xi, m, xi, m, 1, d)) return s;
+        const double xni = d[0].real();
+        double xnp = 0.0;
+        for (int j = 0; j < i; ++j) {
+          if (int s = coldots(x + (size_t)j * m, m, xi, m, 1, d)) return s;
+          const zc prod = d[0];
+          xnp += std::norm(prod);
+          if (int s = axpy1(x + (size_t)j * m, xi, prod)) return s;
+          if (also)
+            if (int s = axpy1(hx + (size_t)j * m, hxi, prod)) return s;
+        }
+        if (xnp > C0P9999 * xni) {
+          for (int j = 0; j < i; ++j) {
+            if (int s = coldots(x + (size_t)j * m, m, xi, m, 1, d)) return s;
+            if (int s = axpy1(x + (size_t)j * m, xi, d[0])) return s;
+            if (also)
+              if (int s = axpy1(hx + (size_t)j * m, hxi, d[0])) return s;
+          }
+        }
+      }
+      if (int s = coldots(xi, m, xi, m, 1, d)) return s;
+      double suma = d[0].real();
+      if (xscl[i] > peq) {
+        if (suma < eps * xscl[i]) {
+          suma = 0.0;
+          irow[i] = 0;
+        } else {
+          suma = 1.0 / sqrt(suma);
+        }
+      } else {
+        suma = 0.0;
+        irow[i] = 0;
+      }
+      std::vector<double> sv(1, suma);
+      if (int s = colscale(xi, m, 1, sv)) return s;
+      if (also)
+        if (int s = colscale(hxi, m, 1, sv)) return s;
+    }
+    return kOk;
+  }
+
+  int grsch_mm(bool also, Z* x, Z* hx, int nvec, int* irow, const double* xscl) {
+    if (nvec <= 10) return grsch_mod(also, x, hx, nvec, irow, xscl);
+    const int nn = nvec / 2, nn2 = nvec - nn;
+    if (int s = grsch_mm(also, x, hx, nn, irow, xscl)) return s;
+    std::vector<zc> xn;
+    if (int s = coldots(x + (size_t)nn * m, m, x + (size_t)nn * m, m, nn2, xn)) return s;
+    if (int s = smallA.ensure(sizeof(Z) * (size_t)nn * nn2)) return s;
+    Z* t = (Z*)smallA.p;
+    if (int s = gemm(CUBLAS_OP_C, CUBLAS_OP_N, nn, nn2, m, one, x, m, x + (size_t)nn * m, m, zero, t, nn, "grsch_mm t"))
+      return s;
+    if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_N, m, nn2, nn, mone, x, m, t, nn, one, x + (size_t)nn * m, m, "grsch_mm x"))
+      return s;
+    if (also)
+      if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_N, m, nn2, nn, mone, hx, m, t, nn, one, hx + (size_t)nn * m, m,
+                       "grsch_mm hx"))
+        return s;
+    std::vector<Z> th((size_t)nn * nn2);
+    if (int s = ck(cudaMemcpyAsync(th.data(), t, sizeof(Z) * th.size(), cudaMemcpyDeviceToHost, st), "grsch_mm t"))
+      return s;
+    if (int s = ck(cudaStreamSynchronize(st), "grsch_mm")) return s;
+    bool rep = false;
+    for (int n = 0; n < nn2; ++n) {
+      double xs = 0;
+      for (int i = 0; i < nn; ++i) xs += th[(size_t)n * nn + i].x * th[(size_t)n * nn + i].x +
+                                         th[(size_t)n * nn + i].y * th[(size_t)n * nn + i].y;
+      if (xs > C0P9999 * xn[n].real()) rep = true;
+    }
+    if (rep) {
+      if (int s = gemm(CUBLAS_OP_C, CUBLAS_OP_N, nn, nn2, m, one, x, m, x + (size_t)nn * m, m, zero, t, nn,
+                       "grsch_mm t2"))
+        return s;
+      if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_N, m, nn2, nn, mone, x, m, t, nn, one, x + (size_t)nn * m, m,
+                       "grsch_mm x2"))
+        return s;
+      if (also)
+        if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_N, m, nn2, nn, mone, hx, m, t, nn, one, hx + (size_t)nn * m, m,
+                         "grsch_mm hx2"))
+          return s;
+    }
+    return grsch_mm(also, x + (size_t)nn * m, also ? hx + (size_t)nn * m : nullptr, nn2, irow + nn, xscl + nn);
+  }
+
+  // orthonormalise columns [nconv, nvec) of x (ld m) against [0, nconv) twice and among themselves
+  int grsch_loop(bool also, Z* x, Z* hx, int nconv, int nvec, std::vector<int>& irow) {
+    irow.assign(std::max(nvec, 0), 1);
+    if (nvec <= nconv) return kOk;
+    const int k = nvec - nconv;
+    std::vector<zc> d;
+    if (int s = coldots(x + (size_t)nconv * m, m, x + (size_t)nconv * m, m, k, d)) return s;
+    std::vector<double> xscl(k);
+    for (int i = 0; i < k; ++i) xscl[i] = d[i].real();
+    if (nconv > 0) {
+      if (int s = smallA.ensure(sizeof(Z) * (size_t)nconv * k)) return s;
+      Z* t = (Z*)smallA.p;
+      for (int pass = 0; pass < 2; ++pass) {
+        if (int s = gemm(CUBLAS_OP_C, CUBLAS_OP_N, nconv, k, m, one, x, m, x + (size_t)nconv * m, m, zero, t, nconv,
+                         "grsch_loop t"))
+          return s;
+        if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_N, m, k, nconv, mone, x, m, t, nconv, one, x + (size_t)nconv * m, m,
+                         "grsch_loop x"))
+          return s;
+        if (also)
+          if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_N, m, k, nconv, mone, hx, m, t, nconv, one, hx + (size_t)nconv * m,
+                           m, "grsch_loop hx"))
+            return s;
+      }
+    }
+    return grsch_mm(also, x + (size_t)nconv * m, also ? hx + (size_t)nconv * m : nullptr, k, irow.data() + nconv,
+                    xscl.data());
+  }
+
+  int grsch_shift(Z* x, long long ldx, int nconv, int nvec, const std::vector<int>& irow, int* ired) {
+    int j = nconv;
+    *ired = 0;
+    for (int n = nconv; n < nvec; ++n) {
+      if (irow[n] == 0) {
+        ++*ired;
+      } else {
+        if (j < n)
+          if (int s = copycols(x + (size_t)j * ldx, ldx, x + (size_t)n * ldx, ldx, 1)) return s;
+        ++j;
+      }
+    }
+    return kOk;
+  }
+
+  // psi/hpsi live with leading dimension ldp; the GS routines work on ld m, so
+  // when ldp != m the block is staged through bas-sized scratch (dvec).
+  int rayleigh(int lo, int hi, std::vector<double>& eg, std::vector<double>& res) {
+    const int n = hi - lo;
+    if (n <= 0) return kOk;
+    if (int s = dvec.ensure(sizeof(double) * 2 * n)) return s;
+    double* e = (double*)dvec.p;
+    k_rayleigh_residual<<<n, kColThreads, 0, st>>>(m, Pc(lo), ldp, HPc(lo), ldp, e, e + n);
+    std::vector<double> h(2 * n);
+    if (int s = ck(cudaMemcpyAsync(h.data(), e, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, st), "rayleigh"))
+      return s;
+    if (int s = ck(cudaStreamSynchronize(st), "rayleigh")) return s;
+    for (int i = 0; i < n; ++i) {
+      eg[lo + i] = h[i];
+      res[lo + i] = h[n + i];
+    }
+    return kOk;
+  }
+
+  double xmax_error(int neig) {
+    std::vector<double> eg(neig), res(neig);
+    if (rayleigh(0, neig, eg, res)) return -1.0;
+    double x = 0;
+    for (int i = 0; i < neig; ++i) x = std::max(x, res[i]);
+    return x;
+  }
+};
+
+struct Trim {
+  std::vector<double>* eg;
+  int nconv, niter;
+  double epsa;
+  // the 'adjusts ntst for degeneracies' loop (ditsp_c16_loop.f90:263-290); the
+  // trip count is fixed on entry, as a Fortran DO loop's
+  int degeneracy(int ntst) const {
+    const int trips = ntst - nconv + 1;
+    for (int it = 0; it < trips; ++it) {
+      double emax = (*eg)[nconv];
+      for (int n = nconv; n < ntst; ++n) emax = std::max(emax, (*eg)[n]);
+      double emin = emax + 10.0 * epsa;
+      for (int n = ntst; n < niter; ++n) emin = std::min(emin, (*eg)[n]);
+      if (emax + epsa > emin) {
+        --ntst;
+        if (ntst <= nconv) break;
+      }
+    }
+    return ntst;
+  }
+};
+
+}  // namespace
+
+// The driver. psi/hpsi: device complex128 (ldp >= mtxd), mxdbnd columns.
+// hamsm: host complex(8) (mxdsml, mxdsml) column-major (first mtxds used).
+// hdiag: host real(mtxd). ei: host real(mxdbnd).
+int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, double epspsi, int* neig_io, int mtxds,
+                 void* psi, long long ldp, void* hpsi, const double* hamsm, int mxdsml, const double* hdiag,
+                 int mxdbnd, double* ei, long long* ihkpsum, cudaStream_t st) {
+  if (!c->have_basis || !c->have_pot) return fail(kNotReady, "ditsp_c16: basis and potential must be set");
+  const int mtxd = c->mtxd;
+  int neig = *neig_io;
+  *ifail = 0;
+  *ihkpsum = 0;
+  if (neig < 1) return kOk;
+  if (neig > mtxds) return fail(kBadArg, "ditsp_c16: neig is greater than mtxds");
+  if (neig > mxdbnd) return fail(kBadArg, "ditsp_c16: neig is greater than mxdbnd");
+  if (3 * neig > mxdsml) return fail(kBadArg, "ditsp_c16: 3*neig is greater than mxdsml");
+  if (mtxds > mxdsml) return fail(kBadArg, "ditsp_c16: mtxds is greater than mxdsml");
+  if (ldp < mtxd) return fail(kBadArg, "ditsp_c16: leading dimension smaller than mtxd");
+
+  Solver S;
+  S.c = c;
+  S.st = st;
+  S.blas = c->blas;
+  cublasSetStream(S.blas, st);
+  S.m = mtxd;
+  S.mxdsml = mxdsml;
+  S.mxdbnd = mxdbnd;
+  S.ldp = ldp;
+  S.P = (Z*)psi;
+  S.HP = (Z*)hpsi;
+  int s;
+  if ((s = S.eg_d.ensure(sizeof(double) * (size_t)std::max(mxdsml, 1)))) return s;
+
+  // upload hamsm (leading mtxds block) once
+  auto load_small = [&](DevBuf& buf, int n) -> int {
+    int r = buf.ensure(sizeof(Z) * (size_t)n * n);
+    if (r) return r;
+    return S.ck(cudaMemcpy2DAsync(buf.p, sizeof(Z) * n, hamsm, sizeof(Z) * (size_t)mxdsml, sizeof(Z) * n, n,
+                                  cudaMemcpyHostToDevice, st),
+                "hamsm upload");
+  };
+
+  std::vector<double> eg(std::max(mtxd, mxdsml) + 2, 0.0), work(mxdsml + 2, 0.0);
+  std::vector<double> et;
+
+  if (mtxds >= mtxd) {
+    // non-iterative diagonalisation (ditsp_c16.f90:218-232)
+    if ((s = load_small(S.smallV, mtxds))) return s;
+    if ((s = S.diag((Z*)S.smallV.p, mtxds, et))) return s;
+    if ((s = S.copycols(S.P, ldp, (Z*)S.smallV.p, mtxds, neig))) return s;
+    for (int i = 0; i < neig; ++i) ei[i] = et[i];
+    return S.ck(cudaStreamSynchronize(st), "ditsp");
+  }
+
+  if ((s = S.bas.ensure(sizeof(Z) * (size_t)mtxd * mxdsml))) return s;
+  if ((s = S.hbas.ensure(sizeof(Z) * (size_t)mtxd * mxdsml))) return s;
+  if ((s = S.ck(cudaMemsetAsync(S.bas.p, 0, sizeof(Z) * (size_t)mtxd * mxdsml, st), "bas"))) return s;
+  if ((s = S.hdiag_d.ensure(sizeof(double) * mtxd))) return s;
+  if ((s = S.ck(cudaMemcpyAsync(S.hdiag_d.p, hdiag, sizeof(double) * mtxd, cudaMemcpyHostToDevice, st), "hdiag")))
+    return s;
+
+  // ---- start (ditsp_c16_start.f90) ----
+  if ((s = load_small(S.smallV, mtxds))) return s;
+  if ((s = S.diag((Z*)S.smallV.p, mtxds, et))) return s;
+  double epsa = std::max(epspsi, fabs((et[neig - 1] - et[0]) / (double)(50 * neig)));
+  int ndeg = neig;
+  for (int i = neig; i < mtxds; ++i) {
+    if (fabs(et[i] - et[i - 1]) > epsa) break;
+    ndeg = i + 1;
+  }
+  ndeg = std::min(ndeg, mxdbnd);
+  int niter = ndeg + 1;
+  if (niter < mtxds) {
+    for (int i = ndeg + 1; i < mtxds; ++i) {
+      if (fabs(et[i] - et[i - 1]) > epsa) break;
+      niter = i + 1;
+    }
+  } else {
+    niter = mtxds;
+  }
+  niter = std::min(niter, mxdbnd);
+  int nexact = neig;
+  const double ecut = C1P2 * et[neig - 1] - C0P2 * et[0];
+  for (int i = neig; i < mtxds; ++i) {
+    if (et[i] > ecut) break;
+    nexact = i + 1;
+  }
+  nexact = std::min(std::min(nexact, mxdsml / 3), std::min(neig + 2 + neig / 5, mtxds / 2)) + 3;
+  {
+    const int imax = nexact - 1;
+    for (int i = 1; i <= imax; ++i) {
+      --nexact;
+      if (fabs(et[imax - i + 1] - et[imax - i]) > epsa) break;
+    }
+  }
+  nexact = std::max(niter, nexact);
+  if (nexact + niter + niter / 5 + 2 > mxdsml) return fail(kBadArg, "ditsp_c16_start: increase mxdsml");
+  // bas(:, 1:nexact) = small eigenvectors zero-padded; hbas = H bas
+  if ((s = S.ck(cudaMemcpy2DAsync(S.bas.p, sizeof(Z) * mtxd, S.smallV.p, sizeof(Z) * mtxds, sizeof(Z) * mtxds, nexact,
+                                  cudaMemcpyDeviceToDevice, st),
+                "start basis")))
+    return s;
+  if ((s = S.hk(S.B(0), mtxd, S.HB(0), mtxd, nexact))) return s;
+  int nitold;
+  bool lortho;
+  if (iguess != 1) {
+    if ((s = S.copycols(S.P, ldp, S.B(0), mtxd, niter))) return s;
+    if ((s = S.copycols(S.HP, ldp, S.HB(0), mtxd, niter))) return s;
+    lortho = true;
+    nitold = 0;
+  } else {
+    if ((s = S.hk(S.P, ldp, S.HP, ldp, neig))) return s;
+    if ((s = S.copycols(S.B(nexact), mtxd, S.P, ldp, neig))) return s;
+    if ((s = S.copycols(S.HB(nexact), mtxd, S.HP, ldp, neig))) return s;
+    lortho = false;
+    nitold = neig;
+    if (niter > neig) {
+      if ((s = S.copycols(S.Pc(neig), ldp, S.B(neig), mtxd, niter - neig))) return s;
+      if ((s = S.copycols(S.HPc(neig), ldp, S.HB(neig), mtxd, niter - neig))) return s;
+    }
+  }
+
+  // P/HP are handled by the GS routines with leading dimension m: stage them
+  // through a packed copy when ldp != m.
+  DevBuf pk, hpk;
+  const bool packed = ldp != mtxd;
+  Z* PP = S.P;
+  Z* HPP = S.HP;
+  if (packed) {
+    if ((s = pk.ensure(sizeof(Z) * (size_t)mtxd * mxdbnd)) || (s = hpk.ensure(sizeof(Z) * (size_t)mtxd * mxdbnd)))
+      return s;
+    if ((s = S.copycols((Z*)pk.p, mtxd, S.P, ldp, mxdbnd)) || (s = S.copycols((Z*)hpk.p, mtxd, S.HP, ldp, mxdbnd)))
+      return s;
+    PP = (Z*)pk.p;
+    HPP = (Z*)hpk.p;
+    S.P = PP;
+    S.HP = HPP;
+    S.ldp = mtxd;
+  }
+
+  int nconv = 0;
+  bool lsafe = false, lconv = false;
+  double xmax = 1.0;
+  int mcref = 2;
+  int iseed = -1;
+  // ran2 state (Src/numeric/ran2.f90), re-initialised by the negative seed
+  int ir[97];
+  int iy = 0, iff = 0;
+  auto ran2 = [&](int& idum) -> double {
+    const int M = 714025, IA = 1366, IC = 150889;
+    if (idum < 0 || iff == 0) {
+      iff = 1;
+      idum = (IC - idum) % M;
+      for (int j = 0; j < 97; ++j) {
+        idum = (int)(((long long)IA * idum + IC) % M);
+        ir[j] = idum;
+      }
+      idum = (int)(((long long)IA * idum + IC) % M);
+      iy = idum;
+    }
+    const int j = (int)((97LL * iy) / M);
+    iy = ir[j];
+    const double v = iy * 1.4005111865831e-6;
+    idum = (int)(((long long)IA * idum + IC) % M);
+    ir[j] = idum;
+    return v;
+  };
+
+  auto compact_eg = [&](const std::vector<int>& irow, int lo, int hi) {
+    int n = lo;
+    for (int nac = lo; nac < hi; ++nac) {
+      if (irow[nac] != 0) {
+        if (n < nac) {
+          eg[n] = eg[nac];
+          work[n] = work[nac];
+        }
+        ++n;
+      }
+    }
+  };
+  auto first_unconverged = [&](int nmax, double tol) {
+    int ntst = nconv;
+    for (int n = nconv; n < nmax; ++n) {
+      if (work[n] > tol) break;
+      ntst = n + 1;
+    }
+    return ntst;
+  };
+
+  std::vector<int> irow;
+  for (int ic = 1; ic <= icmax; ++ic) {
+    const int mcmax = mcref;
+    bool lexit = false;
+    lconv = false;
+    for (int mc = 1; mc <= mcmax; ++mc) {
+      // ---- ditsp_c16_loop ----
+      lconv = false;
+      lexit = false;
+      if ((s = S.rayleigh(nconv, niter, eg, work))) return s;
+      const double xmold = xmax;
+      xmax = 0.0;
+      for (int n = nconv; n < std::min(ndeg, niter); ++n) xmax = std::max(xmax, work[n]);
+      if (ipr > 3)
+        printf("  ditsp_c16_loop ic = %d  mc = %d  nconv = %d  niter = %d  xmax = %.6e\n", ic, mc, nconv, niter, xmax);
+      if (mc > 1 && xmax > C0P2 * xmold) {
+        mcref = mc;
+        lexit = true;
+      }
+      if (!lexit && xmax < epspsi * epspsi && lsafe && niter >= ndeg) {
+        if (lortho) {
+          neig = ndeg;
+          lconv = true;
+        } else {
+          if ((s = S.grsch_loop(true, PP, HPP, nconv, niter, irow))) return s;
+          int ired;
+          if ((s = S.grsch_shift(PP, mtxd, nconv, niter, irow, &ired))) return s;
+          if ((s = S.grsch_shift(HPP, mtxd, nconv, niter, irow, &ired))) return s;
+          if (ired > 0) lsafe = false;
+          compact_eg(irow, nconv, niter);
+          niter -= ired;
+          lortho = true;
+          if (nconv < niter) {
+            xmax = 0.0;
+            for (int n = nconv; n < std::min(niter, ndeg); ++n) xmax = std::max(xmax, work[n]);
+            if (xmax < epspsi * epspsi && lsafe && niter >= ndeg) {
+              neig = ndeg;
+              lconv = true;
+            }
+          }
+        }
+      }
+      if (!lconv && !lexit && niter == nconv) lexit = true;
+      const double tol = C0P01 * epspsi * epspsi;
+      int ntst = nconv;
+      if (!lconv && !lexit) {
+        ntst = first_unconverged(niter, tol);
+        if (ntst > nconv) ntst = Trim{&eg, nconv, niter, epsa}.degeneracy(ntst);
+      }
+      if (!lconv && !lexit && ntst > nconv && !lortho) {
+        if ((s = S.grsch_loop(true, PP, HPP, nconv, ntst, irow))) return s;
+        irow.resize(std::max(niter, ntst), 1);
+        for (int n = ntst; n < niter; ++n) irow[n] = 1;
+        int ired;
+        if ((s = S.grsch_shift(PP, mtxd, nconv, niter, irow, &ired))) return s;
+        if ((s = S.grsch_shift(HPP, mtxd, nconv, niter, irow, &ired))) return s;
+        if (ired > 0) lsafe = false;
+        compact_eg(irow, nconv, niter);
+        lortho = true;
+        ntst -= ired;
+        niter -= ired;
+        if (ntst > nconv) {
+          const int nmax = ntst;
+          ntst = first_unconverged(nmax, tol);
+          if (ntst > nconv) ntst = Trim{&eg, nconv, niter, epsa}.degeneracy(ntst);
+        }
+      }
+      if (!lconv && !lexit && niter == nconv) lexit = true;
+      if (!lconv && !lexit && ntst > nconv) {
+        // span test against the previous basis vectors (ditsp_c16_loop.f90:396-461)
+        const int k = ntst - nconv;
+        if ((s = S.smallA.ensure(sizeof(Z) * (size_t)k * k))) return s;
+        if ((s = S.gemm(CUBLAS_OP_C, CUBLAS_OP_N, k, k, mtxd, S.one, S.B(nexact + nconv), mtxd, PP + (size_t)nconv * mtxd,
+                        mtxd, S.zero, (Z*)S.smallA.p, k, "span test")))
+          return s;
+        std::vector<Z> vs((size_t)k * k);
+        if ((s = S.ck(cudaMemcpyAsync(vs.data(), S.smallA.p, sizeof(Z) * vs.size(), cudaMemcpyDeviceToHost, st), "span")))
+          return s;
+        if ((s = S.ck(cudaStreamSynchronize(st), "span"))) return s;
+        bool done = false;
+        for (int it = 0; it < 10 * mxdbnd && !done; ++it) {
+          const int nmax = ntst;
+          ntst = nconv;
+          bool lxn = false;
+          for (int n = 0; n < nmax - nconv; ++n) {
+            double xn = 0;
+            for (int i = 0; i < nmax - nconv; ++i)
+              xn += vs[(size_t)n * k + i].x * vs[(size_t)n * k + i].x + vs[(size_t)n * k + i].y * vs[(size_t)n * k + i].y;
+            if (xn < C0P95) {
+              lxn = true;
+              break;
+            }
+            ntst = nconv + n + 1;
+          }
+          if (lxn) {
+            if (ntst <= nconv) done = true;
+          } else {
+            double emax = eg[nconv];
+            for (int n = nconv; n < ntst; ++n) emax = std::max(emax, eg[n]);
+            double emin = emax + 10.0 * epsa;
+            for (int n = ntst; n < niter; ++n) emin = std::min(emin, eg[n]);
+            if (emax + epsa > emin) {
+              --ntst;
+              if (ntst <= nconv) done = true;
+            } else {
+              done = true;
+            }
+          }
+          if (!done && it == 10 * mxdbnd - 1) return fail(kBadArg, "ditsp_c16_loop: span test did not terminate");
+        }
+      }
+      if (!lconv && !lexit) {
+        if (ntst > nconv) {
+          if ((s = S.copycols(S.B(nexact + nconv), mtxd, PP + (size_t)nconv * mtxd, mtxd, ntst - nconv))) return s;
+          std::vector<int> irowb;
+          if ((s = S.grsch_loop(false, (Z*)S.bas.p, (Z*)S.hbas.p, nexact + nconv, nexact + ntst, irowb))) return s;
+          int ired;
+          if ((s = S.grsch_shift((Z*)S.bas.p, mtxd, nexact + nconv, nexact + ntst, irowb, &ired))) return s;
+          if (ired > 0) {
+            lsafe = false;
+            std::vector<int> ir2(niter, 1);
+            for (int n = nconv; n < ntst; ++n) ir2[n] = irowb[nexact + n];
+            int r2;
+            if ((s = S.grsch_shift(PP, mtxd, nconv, niter, ir2, &r2))) return s;
+            if ((s = S.grsch_shift(HPP, mtxd, nconv, niter, ir2, &r2))) return s;
+            compact_eg(ir2, nconv, niter);
+          }
+          const int nnew = ntst - ired - nconv;
+          if ((s = S.hk(S.B(nexact + nconv), mtxd, S.HB(nexact + nconv), mtxd, nnew))) return s;
+          nconv = ntst - ired;
+          niter -= ired;
+        }
+        // relaxation step
+        const int nr = niter - nconv;
+        if (nr > 0) {
+          if ((s = S.dvec2.ensure(sizeof(double) * nr))) return s;
+          if ((s = S.ck(cudaMemcpyAsync(S.dvec2.p, eg.data() + nconv, sizeof(double) * nr, cudaMemcpyHostToDevice, st),
+                        "eg")))
+            return s;
+          dim3 g((unsigned)std::min(64, (mtxd + 255) / 256), nr);
+          k_jacobi<<<g, 256, 0, st>>>(mtxd, PP + (size_t)nconv * mtxd, mtxd, HPP + (size_t)nconv * mtxd, mtxd,
+                                      (const double*)S.dvec2.p, (const double*)S.hdiag_d.p);
+          std::vector<zc> nrm;
+          if ((s = S.coldots(PP + (size_t)nconv * mtxd, mtxd, PP + (size_t)nconv * mtxd, mtxd, nr, nrm))) return s;
+          std::vector<double> sc(nr);
+          for (int i = 0; i < nr; ++i) sc[i] = 1.0 / sqrt(nrm[i].real());
+          if ((s = S.colscale(PP + (size_t)nconv * mtxd, mtxd, nr, sc))) return s;
+          lortho = false;
+          if ((s = S.hk(PP + (size_t)nconv * mtxd, mtxd, HPP + (size_t)nconv * mtxd, mtxd, nr))) return s;
+        }
+      }
+      if (lexit || lconv) break;
+    }
+    if (!lsafe) mcref = 3;
+    // ---- ditsp_c16_ritz ----
+    lconv = false;
+    int nsize = nexact + nitold + niter - nconv;
+    const int nlow = nexact + nitold - nconv;
+    if (nsize > mxdsml) return fail(kBadArg, "ditsp_c16_ritz: change mxdsml");
+    if (nconv < niter)
+      if ((s = S.copycols(S.B(nlow + nconv), mtxd, PP + (size_t)nconv * mtxd, mtxd, niter - nconv))) return s;
+    if (!lsafe || niter == nconv) {
+      ++nsize;
+      if (nsize > mxdsml) return fail(kBadArg, "ditsp_c16_ritz: change mxdsml");
+      std::vector<Z> rv(mtxd);
+      for (int k = 0; k < mtxd; ++k) {
+        const double xr = ran2(iseed);
+        const double xi = ran2(iseed);
+        rv[k] = make_cuDoubleComplex(xr, xi);
+      }
+      if ((s = S.ck(cudaMemcpyAsync(S.B(nsize - 1), rv.data(), sizeof(Z) * mtxd, cudaMemcpyHostToDevice, st), "ran")))
+        return s;
+      if ((s = S.ck(cudaStreamSynchronize(st), "ran"))) return s;
+    }
+    {
+      std::vector<int> irowb;
+      if ((s = S.grsch_loop(false, (Z*)S.bas.p, (Z*)S.hbas.p, nexact + nconv, nsize, irowb))) return s;
+      int ired;
+      if ((s = S.grsch_shift((Z*)S.bas.p, mtxd, nexact + nconv, nsize, irowb, &ired))) return s;
+      nsize -= ired;
+    }
+    if (nsize > mtxd) return fail(kBadArg, "ditsp_c16_ritz: problems with Gram-Schmidt");
+    const int lo = nexact + nconv;
+    if ((s = S.hk(S.B(lo), mtxd, S.HB(lo), mtxd, nsize - lo))) return s;
+    if ((s = S.smallV.ensure(sizeof(Z) * (size_t)nsize * nsize))) return s;
+    if ((s = S.gemm(CUBLAS_OP_C, CUBLAS_OP_N, nsize, nsize, mtxd, S.one, (Z*)S.hbas.p, mtxd, (Z*)S.bas.p, mtxd, S.zero,
+                    (Z*)S.smallV.p, nsize, "ritz hamsm")))
+      return s;
+    std::vector<double> egs;
+    if ((s = S.diag((Z*)S.smallV.p, nsize, egs))) return s;
+    for (int i = 0; i < nsize; ++i) eg[i] = egs[i];
+    ndeg = neig;
+    for (int i = neig; i < nsize; ++i) {
+      if (fabs(eg[i] - eg[i - 1]) > epsa) break;
+      ndeg = i + 1;
+    }
+    ndeg = std::min(ndeg, mxdbnd);
+    niter = ndeg + 1;
+    if (nsize > niter) {
+      for (int i = ndeg + 1; i < nsize; ++i) {
+        if (fabs(eg[i] - eg[i - 1]) > epsa) break;
+        niter = i + 1;
+      }
+    }
+    {
+      const int nmax = (mxdsml - nexact + nconv) / 2;
+      niter = std::min(std::min(niter, nmax), std::min(nexact, mxdbnd));
+      niter = std::max(niter, ndeg);
+    }
+    if (nconv > 0) {
+      std::vector<Z> vh((size_t)nsize * nsize);
+      if ((s = S.ck(cudaMemcpyAsync(vh.data(), S.smallV.p, sizeof(Z) * vh.size(), cudaMemcpyDeviceToHost, st), "vsm")))
+        return s;
+      if ((s = S.ck(cudaStreamSynchronize(st), "vsm"))) return s;
+      const int kmax = nconv;
+      for (int k = 0; k < kmax; ++k) {
+        const int nmax = nconv;
+        nconv = 0;
+        bool ljump = true;
+        for (int n = 0; n < nmax; ++n) {
+          double xn = 0;
+          for (int i = 0; i < nexact + nmax; ++i)
+            xn += vh[(size_t)n * nsize + i].x * vh[(size_t)n * nsize + i].x +
+                  vh[(size_t)n * nsize + i].y * vh[(size_t)n * nsize + i].y;
+          if (xn < C0P99) {
+            ljump = false;
+            break;
+          }
+          nconv = n + 1;
+        }
+        if (ljump && fabs(eg[nconv] - eg[nconv - 1]) < epsa) {
+          --nconv;
+          ljump = false;
+        }
+        if (ljump || nconv == 0) break;
+      }
+    }
+    if ((s = S.gemm(CUBLAS_OP_N, CUBLAS_OP_N, mtxd, niter, nsize, S.one, (Z*)S.bas.p, mtxd, (Z*)S.smallV.p, nsize,
+                    S.zero, PP, mtxd, "ritz psi")))
+      return s;
+    if ((s = S.gemm(CUBLAS_OP_N, CUBLAS_OP_N, mtxd, niter, nsize, S.one, (Z*)S.hbas.p, mtxd, (Z*)S.smallV.p, nsize,
+                    S.zero, HPP, mtxd, "ritz hpsi")))
+      return s;
+    if (niter > nconv) {
+      if ((s = S.copycols(S.B(nexact + nconv), mtxd, PP + (size_t)nconv * mtxd, mtxd, niter - nconv))) return s;
+      if ((s = S.copycols(S.HB(nexact + nconv), mtxd, HPP + (size_t)nconv * mtxd, mtxd, niter - nconv))) return s;
+    }
+    if (nconv >= ndeg) neig = ndeg;
+    xmax = S.xmax_error(neig);
+    if (xmax < 0) return fail(kCuda, "ditsp_c16: residual evaluation failed");
+    if (ipr > 2)
+      printf("  ditsp_c16_ritz ic = %d  nconv = %d  niter = %d  nsize = %d  ndeg = %d  xmax = %.6e  e1 = %.12f\n", ic,
+             nconv, niter, nsize, ndeg, xmax, eg[0]);
+    lconv = xmax < epspsi * epspsi;
+    if (lconv) break;
+    nitold = niter;
+    lortho = true;
+    lsafe = true;
+    if (xmax < C0P01) mcref = std::min(mcref + 2, 8);
+  }
+  if (!lconv) {
+    *ifail = 1 + (int)(-log10(xmax));
+    if (*ifail == 0) *ifail = 1;
+  }
+  for (int i = 0; i < neig; ++i) ei[i] = eg[i];
+  *neig_io = neig;
+  *ihkpsum = S.ihk;
+  if (packed) {
+    if ((s = S.ck(cudaMemcpy2DAsync(psi, ldp * sizeof(Z), PP, mtxd * sizeof(Z), mtxd * sizeof(Z), mxdbnd,
+                                    cudaMemcpyDeviceToDevice, st),
+                  "unpack")))
+      return s;
+    if ((s = S.ck(cudaMemcpy2DAsync(hpsi, ldp * sizeof(Z), HPP, mtxd * sizeof(Z), mtxd * sizeof(Z), mxdbnd,
+                                    cudaMemcpyDeviceToDevice, st),
+                  "unpack")))
+      return s;
+  }
+  if (S.sol) cusolverDnDestroy(S.sol);
+  S.sol = nullptr;
+  if ((s = S.ck(cudaStreamSynchronize(st), "ditsp"))) return s;
+  return lconv ? kOk : kNotConverged;
+}
+
+}  // namespace cpwb

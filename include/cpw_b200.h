@@ -10,6 +10,7 @@
  *     reference's leading dimensions, 1-based isort into kgv(3, mxdgve):
  *       cpw_b200_hk_psi_c16  / hk_psi_c16_    replaces Src/hk_psi/reference/hk_psi_c16.f90:28-32
  *       cpw_b200_hk_psi_nl_c16 / hk_psi_nl_c16_ replaces Src/cpw_lib/hk_psi_nl_c16.f90:23-24
+ *       cpw_b200_ditsp_c16   / ditsp_c16_     replaces Src/ditsp/ditsp_c16.f90:20-27
  *     The cpw_b200_* forms return a status (0 = success) and never stop the
  *     program; the trailing-underscore forms are link-time substitutes for the
  *     Fortran symbols and, like the reference, print the message and stop the
@@ -117,6 +118,32 @@ int cpw_b200_hk_psi_nl_c16(const int* mtxd, const int* neig, const double* psi, 
 void hk_psi_nl_c16_(const int* mtxd, const int* neig, const double* psi, double* hpsi, const double* anlga,
                     const double* xnlkb, const int* nanl, const int* ladd, const int* mxddim, const int* mxdbnd,
                     const int* mxdanl);
+
+/* Block iterative eigensolver on device-resident psi/hpsi (complex128, ldpsi >= mtxd,
+ * mxdbnd columns), restating Src/ditsp/ditsp_c16.f90 (start/loop/ritz, block
+ * Gram-Schmidt, zheevd subspace eigensolve, Jacobi relaxation). hamsm is the host
+ * complex(8) (mxdsml, mxdsml) leading block of H, hdiag the host diagonal, ei
+ * host output (mxdbnd). *neig may grow to the degeneracy-closed count. Returns
+ * CPW_B200_NOT_CONVERGED with *ifail = number of accurate digits when epspsi is
+ * not reached in icmax outer iterations. ihkpsum (may be NULL) receives the
+ * number of H|psi> band applications. Synchronous. */
+int cpw_b200_ditsp_device(cpw_b200_ctx* ctx, int ipr, int* ifail, int icmax, int iguess, double epspsi, int* neig,
+                          int mtxds, void* psi, long long ldpsi, void* hpsi, double* ei, const double* hamsm,
+                          int mxdsml, const double* hdiag, int mxdbnd, long long* ihkpsum, void* stream);
+
+/* Src/ditsp/ditsp_c16.f90:20-27 with host arrays (psi, hpsi complex(8) (mxddim, mxdbnd)). */
+int cpw_b200_ditsp_c16(const int* ipr, int* ifail, const int* icmax, const int* iguess, const double* epspsi,
+                       int* lnewanl, int* neig, const int* mtxd, const int* mtxds, double* psi, double* hpsi,
+                       double* ei, const double* ekpg, const int* isort, const double* vscr, const int* kmscr,
+                       const int* ng, const int* kgv, const double* anlga, const double* xnlkb, const int* nanl,
+                       const double* hamsm, const double* hdiag, const int* mxddim, const int* mxdsml,
+                       const int* mxdbnd, const int* mxdgve, const int* mxdscr, const int* mxdanl);
+void ditsp_c16_(const int* ipr, int* ifail, const int* icmax, const int* iguess, const double* epspsi, int* lnewanl,
+                int* neig, const int* mtxd, const int* mtxds, double* psi, double* hpsi, double* ei,
+                const double* ekpg, const int* isort, const double* vscr, const int* kmscr, const int* ng,
+                const int* kgv, const double* anlga, const double* xnlkb, const int* nanl, const double* hamsm,
+                const double* hdiag, const int* mxddim, const int* mxdsml, const int* mxdbnd, const int* mxdgve,
+                const int* mxdscr, const int* mxdanl);
 
 /* ---- allocation-free local H|psi> ----
  * No counterpart in the reference. For callers that cannot call cudaMalloc

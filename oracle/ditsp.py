@@ -324,6 +324,8 @@ def ditsp_c16(hk, neig, mtxd, mtxds, psi, hpsi, hamsm, hdiag, epspsi=1e-5, icmax
             nmax = min(ndeg, niter)
             for n in range(nconv, nmax):
                 xmax = max(xmax, s.work[n])
+            if _TRACE:
+                print(f"  oracle loop ic = {ic}  mc = {mc}  nconv = {nconv}  niter = {niter}  xmax = {xmax:.6e}")
             if mc > 1 and xmax > C_0P2 * xmold:
                 mcref = mc
                 lexit = True
@@ -510,7 +512,9 @@ def ditsp_c16(hk, neig, mtxd, mtxds, psi, hpsi, hamsm, hdiag, epspsi=1e-5, icmax
             lconv = True
         s.nconv, s.niter = nconv, niter
         xmax = ditsp_error(P[:, :neig], HP[:, :neig])
-        if _TRACE: print("ritz", ic, "nconv", nconv, "niter", niter, "nsize", nsize, "xmax", xmax)
+        if _TRACE:
+            print(f"  oracle ritz ic = {ic}  nconv = {nconv}  niter = {niter}  nsize = {nsize}  ndeg = {ndeg}  "
+                  f"xmax = {xmax:.6e}  e1 = {s.eg[0]:.12f}")
         lconv = xmax < epspsi * epspsi
         if lconv:
             break
