@@ -12,6 +12,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <complex>
 #include <string>
 #include <vector>
@@ -115,16 +116,151 @@ __global__ void k_colscale(int m, Z* __restrict__ x, long long ldx, const double
     a[i] = make_cuDoubleComplex(a[i].x * f, a[i].y * f);
 }
 
-// y_j -= c_j x_j  (complex c on device)
-__global__ void k_colaxpy(int m, const Z* __restrict__ x, long long ldx, Z* __restrict__ y, long long ldy,
-                          const Z* __restrict__ c) {
-  const int j = blockIdx.y;
-  const Z f = c[j];
-  const Z* a = x + (size_t)j * ldx;
-  Z* b = y + (size_t)j * ldy;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-    const Z u = a[i];
-    b[i] = make_cuDoubleComplex(b[i].x - (f.x * u.x - f.y * u.y), b[i].y - (f.x * u.y + f.y * u.x));
+// ---------------- device-side modified Gram-Schmidt (<= 10 vectors) ----------------
+// One cooperative launch per block of vectors, restating grsch_mod_c16.f90:77-147
+// with every decision taken on the device: sequential MGS projections, the
+// repeat when xnp > 0.9999 xni, the drop below 1e-20 of the natural scale.
+// Each CTA owns a slice of rows; reductions write per-CTA partial sums to a
+// double-buffered array, pass a grid barrier and are summed in CTA order by
+// every CTA (deterministic, identical in all CTAs).
+struct MgsArgs {
+  int m, nvec, also;
+  Z* x;
+  Z* hx;
+  const double* xscl;
+  int* irow;
+  double* partial;      // 2 * gridDim.x * 4 doubles
+  unsigned* bar;        // [0] arrival count, [1] generation
+  int* err;             // set to 1 when a barrier wait gives up
+  double eps, peq, rep; // 1e-20 (as compiled), tiny/eps, 0.9999
+};
+
+constexpr long long kBarrierSpinLimit = 1LL << 24;   // ~1 s at ~64 ns per try
+
+// Grid barrier with a bounded wait: returns false (and sets *err) if the
+// other CTAs did not arrive in time; all CTAs then leave the kernel.
+__device__ bool grid_barrier(unsigned* bar, int* err) {
+  __syncthreads();
+  __shared__ int ok;
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = bar + 1;
+    const unsigned g = *vgen;
+    __threadfence();
+    ok = 1;
+    if (atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
+      atomicExch(&bar[0], 0u);
+      __threadfence();
+      atomicAdd(&bar[1], 1u);
+    } else {
+      long long it = 0;
+      while (*vgen == g) {
+        if (++it > kBarrierSpinLimit) {
+          atomicExch(err, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(40);
+      }
+    }
+    __threadfence();
+    if (*((volatile int*)err) != 0) ok = 0;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// sums k (<= 4) per-thread values over the grid; result in out[0..k) for every thread
+__device__ bool grid_sum(const MgsArgs& a, int& round, const double* v, int k, double* out, double* sh) {
+  double* buf = a.partial + (size_t)(round & 1) * gridDim.x * 4;
+  for (int t = 0; t < k; ++t) {
+    const double s = block_sum(v[t], sh);
+    if (threadIdx.x == 0) buf[(size_t)blockIdx.x * 4 + t] = s;
+  }
+  ++round;
+  if (!grid_barrier(a.bar, a.err)) return false;
+  for (int t = 0; t < k; ++t) {
+    double s = 0.0;
+    for (unsigned b = 0; b < gridDim.x; ++b) s += ((volatile double*)buf)[(size_t)b * 4 + t];
+    out[t] = s;
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(256) k_mgs(MgsArgs a) {
+  __shared__ double sh[33];
+  const int per = (a.m + gridDim.x - 1) / gridDim.x;
+  const int r0 = blockIdx.x * per, r1 = min(a.m, r0 + per);
+  int round = 0;
+  double v[4], o[4];
+  auto dot = [&](const Z* p, const Z* q, double& re, double& im) {
+    re = 0;
+    im = 0;
+    for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+      const Z u = p[r], w = q[r];
+      re += u.x * w.x + u.y * w.y;
+      im += u.x * w.y - u.y * w.x;
+    }
+  };
+  auto axpy = [&](const Z* p, Z* q, double cr, double ci) {   // q -= c p
+    for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+      const Z u = p[r];
+      q[r] = make_cuDoubleComplex(q[r].x - (cr * u.x - ci * u.y), q[r].y - (cr * u.y + ci * u.x));
+    }
+  };
+  for (int i = 0; i < a.nvec; ++i) {
+    Z* xi = a.x + (size_t)i * a.m;
+    Z* hxi = a.also ? a.hx + (size_t)i * a.m : nullptr;
+    if (i > 0) {
+      double xni = 0, xnp = 0;
+      for (int j = 0; j < i; ++j) {
+        const Z* xj = a.x + (size_t)j * a.m;
+        dot(xj, xi, v[0], v[1]);
+        int k = 2;
+        if (j == 0) {   // xni on the vector before any projection
+          double re, im;
+          dot(xi, xi, re, im);
+          v[2] = re;
+          k = 3;
+        }
+        if (!grid_sum(a, round, v, k, o, sh)) return;
+        if (j == 0) xni = o[2];
+        xnp += o[0] * o[0] + o[1] * o[1];
+        axpy(xj, xi, o[0], o[1]);
+        if (hxi) axpy(a.hx + (size_t)j * a.m, hxi, o[0], o[1]);
+      }
+      if (xnp > a.rep * xni) {
+        for (int j = 0; j < i; ++j) {
+          const Z* xj = a.x + (size_t)j * a.m;
+          dot(xj, xi, v[0], v[1]);
+          if (!grid_sum(a, round, v, 2, o, sh)) return;
+          axpy(xj, xi, o[0], o[1]);
+          if (hxi) axpy(a.hx + (size_t)j * a.m, hxi, o[0], o[1]);
+        }
+      }
+    }
+    double re, im;
+    dot(xi, xi, re, im);
+    v[0] = re;
+    if (!grid_sum(a, round, v, 1, o, sh)) return;
+    double suma = o[0];
+    const double xs = a.xscl[i];
+    int keep = 1;
+    if (xs > a.peq) {
+      if (suma < a.eps * xs) {
+        suma = 0.0;
+        keep = 0;
+      } else {
+        suma = 1.0 / sqrt(suma);
+      }
+    } else {
+      suma = 0.0;
+      keep = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && !keep) a.irow[i] = 0;
+    for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+      xi[r] = make_cuDoubleComplex(xi[r].x * suma, xi[r].y * suma);
+      if (hxi) hxi[r] = make_cuDoubleComplex(hxi[r].x * suma, hxi[r].y * suma);
+    }
   }
 }
 
@@ -143,6 +279,26 @@ struct Solver {
   int lwork = 0;
   long long ihk = 0;
   int status = kOk;
+  // wall-clock accounting per phase (printed when ipr > 1): 0 H|psi>, 1 Gram-Schmidt, 2 subspace eigensolve
+  double tphase[4] = {0, 0, 0, 0};
+  bool timing = false;
+  struct Tick {
+    Solver* s;
+    int k;
+    std::chrono::steady_clock::time_point t0;
+    Tick(Solver* sv, int kk) : s(sv), k(kk) {
+      if (s->timing) {
+        cudaStreamSynchronize(s->st);
+        t0 = std::chrono::steady_clock::now();
+      }
+    }
+    ~Tick() {
+      if (s->timing) {
+        cudaStreamSynchronize(s->st);
+        s->tphase[k] += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      }
+    }
+  };
   const Z one = make_cuDoubleComplex(1, 0), zero = make_cuDoubleComplex(0, 0), mone = make_cuDoubleComplex(-1, 0);
 
   Z* B(int j) { return (Z*)bas.p + (size_t)j * m; }
@@ -157,6 +313,7 @@ struct Solver {
 
   int hk(Z* x, long long ldx, Z* hx, long long ldhx, int n) {
     if (n <= 0) return kOk;
+    Tick tk(this, 0);
     ihk += n;
     return ctx_hkpsi_device(c, n, x, ldx, hx, ldhx, st, true, true);
   }
@@ -197,16 +354,6 @@ struct Solver {
     return ck(cudaStreamSynchronize(st), "colscale");
   }
 
-  // y -= c x for single columns (c host value)
-  int axpy1(const Z* x, Z* y, zc cf) {
-    if (int s = dz.ensure(sizeof(Z) * 8)) return s;
-    Z v = make_cuDoubleComplex(cf.real(), cf.imag());
-    if (int s = ck(cudaMemcpyAsync(dz.p, &v, sizeof(Z), cudaMemcpyHostToDevice, st), "axpy")) return s;
-    dim3 g((unsigned)std::min(64, (m + 255) / 256), 1);
-    k_colaxpy<<<g, 256, 0, st>>>(m, x, m, y, m, (const Z*)dz.p);
-    return ck(cudaStreamSynchronize(st), "axpy");
-  }
-
   int copycols(Z* dst, long long ldd, const Z* src, long long lds, int n) {
     if (n <= 0) return kOk;
     return ck(cudaMemcpy2DAsync(dst, ldd * sizeof(Z), src, lds * sizeof(Z), m * sizeof(Z), n,
@@ -219,6 +366,7 @@ struct Solver {
   int diag(Z* A, int n, std::vector<double>& w) {
     w.assign(n, 0.0);
     if (n <= 0) return kOk;
+    Tick tk(this, 2);
     if (!sol) {
       if (cusolverDnCreate(&sol) != CUSOLVER_STATUS_SUCCESS) return fail(kCusolver, "cusolverDnCreate failed");
     }
@@ -242,52 +390,49 @@ struct Solver {
   }
 
   // ---- block Gram-Schmidt family (grsch_mod / grsch_mm / grsch_loop / grsch_shift) ----
+  // grsch_mod on the device (k_mgs); irow/xscl are host arrays of nvec entries
+  DevBuf mgs_part, mgs_bar, mgs_irow, mgs_xscl;
+  int mgs_grid = 0;
   int grsch_mod(bool also, Z* x, Z* hx, int nvec, int* irow, const double* xscl) {
-    const double eps = CEPS20;
-    const double peq = (1.0 / eps) * 2.2250738585072014e-308;
-    std::vector<zc> d;
-    for (int i = 0; i < nvec; ++i) {
-      Z* xi = x + (size_t)i * m;
-      Z* hxi = also ? hx + (size_t)i * m : nullptr;
-      if (i > 0) {
-        if (int s = coldots(xi, m, xi, m, 1, d)) return s;
-        const double xni = d[0].real();
-        double xnp = 0.0;
-        for (int j = 0; j < i; ++j) {
-          if (int s = coldots(x + (size_t)j * m, m, xi, m, 1, d)) return s;
-          const zc prod = d[0];
-          xnp += std::norm(prod);
-          if (int s = axpy1(x + (size_t)j * m, xi, prod)) return s;
-          if (also)
-            if (int s = axpy1(hx + (size_t)j * m, hxi, prod)) return s;
-        }
-        if (xnp > C0P9999 * xni) {
-          for (int j = 0; j < i; ++j) {
-            if (int s = coldots(x + (size_t)j * m, m, xi, m, 1, d)) return s;
-            if (int s = axpy1(x + (size_t)j * m, xi, d[0])) return s;
-            if (also)
-              if (int s = axpy1(hx + (size_t)j * m, hxi, d[0])) return s;
-          }
-        }
-      }
-      if (int s = coldots(xi, m, xi, m, 1, d)) return s;
-      double suma = d[0].real();
-      if (xscl[i] > peq) {
-        if (suma < eps * xscl[i]) {
-          suma = 0.0;
-          irow[i] = 0;
-        } else {
-          suma = 1.0 / sqrt(suma);
-        }
-      } else {
-        suma = 0.0;
-        irow[i] = 0;
-      }
-      std::vector<double> sv(1, suma);
-      if (int s = colscale(xi, m, 1, sv)) return s;
-      if (also)
-        if (int s = colscale(hxi, m, 1, sv)) return s;
+    if (nvec <= 0) return kOk;
+    if (!mgs_grid) {
+      int dev = 0, nsm = 0, per = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_mgs, 256, 0);
+      mgs_grid = std::max(1, std::min(nsm * std::max(per, 1), nsm));
     }
+    const int grid = std::max(1, std::min(mgs_grid, (m + 511) / 512));
+    int s;
+    if ((s = mgs_part.ensure(sizeof(double) * 8 * (size_t)mgs_grid)) || (s = mgs_bar.ensure(sizeof(unsigned) * 4)) ||
+        (s = mgs_irow.ensure(sizeof(int) * 16)) || (s = mgs_xscl.ensure(sizeof(double) * 16)))
+      return s;
+    if ((s = ck(cudaMemsetAsync(mgs_bar.p, 0, sizeof(unsigned) * 4, st), "mgs"))) return s;
+    if ((s = ck(cudaMemcpyAsync(mgs_irow.p, irow, sizeof(int) * nvec, cudaMemcpyHostToDevice, st), "mgs"))) return s;
+    if ((s = ck(cudaMemcpyAsync(mgs_xscl.p, xscl, sizeof(double) * nvec, cudaMemcpyHostToDevice, st), "mgs")))
+      return s;
+    MgsArgs a;
+    a.m = m;
+    a.nvec = nvec;
+    a.also = also ? 1 : 0;
+    a.x = x;
+    a.hx = hx;
+    a.xscl = (const double*)mgs_xscl.p;
+    a.irow = (int*)mgs_irow.p;
+    a.partial = (double*)mgs_part.p;
+    a.bar = (unsigned*)mgs_bar.p;
+    a.err = (int*)mgs_bar.p + 2;
+    a.eps = CEPS20;
+    a.peq = (1.0 / CEPS20) * 2.2250738585072014e-308;
+    a.rep = C0P9999;
+    void* args[] = {&a};
+    if ((s = ck(cudaLaunchCooperativeKernel((const void*)k_mgs, dim3(grid), dim3(256), args, 0, st), "mgs launch")))
+      return s;
+    int err = 0;
+    if ((s = ck(cudaMemcpyAsync(irow, mgs_irow.p, sizeof(int) * nvec, cudaMemcpyDeviceToHost, st), "mgs"))) return s;
+    if ((s = ck(cudaMemcpyAsync(&err, (int*)mgs_bar.p + 2, sizeof(int), cudaMemcpyDeviceToHost, st), "mgs"))) return s;
+    if ((s = ck(cudaStreamSynchronize(st), "mgs"))) return s;
+    if (err) return fail(kTimeout, "grsch_mod: a grid barrier wait gave up");
     return kOk;
   }
 
@@ -335,6 +480,7 @@ struct Solver {
 
   // orthonormalise columns [nconv, nvec) of x (ld m) against [0, nconv) twice and among themselves
   int grsch_loop(bool also, Z* x, Z* hx, int nconv, int nvec, std::vector<int>& irow) {
+    Tick tk(this, 1);
     irow.assign(std::max(nvec, 0), 1);
     if (nvec <= nconv) return kOk;
     const int k = nvec - nconv;
@@ -458,6 +604,8 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
   S.ldp = ldp;
   S.P = (Z*)psi;
   S.HP = (Z*)hpsi;
+  S.timing = ipr > 1;
+  const auto t_start = std::chrono::steady_clock::now();
   int s;
   if ((s = S.eg_d.ensure(sizeof(double) * (size_t)std::max(mxdsml, 1)))) return s;
 
@@ -893,6 +1041,13 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
                                     cudaMemcpyDeviceToDevice, st),
                   "unpack")))
       return s;
+  }
+  if (ipr > 1) {
+    const double tot = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    printf("  ditsp_c16: %lld H|psi> band products, total %.4f s: H|psi> %.4f s, Gram-Schmidt %.4f s, "
+           "subspace eigensolve %.4f s, other %.4f s\n",
+           S.ihk, tot, S.tphase[0], S.tphase[1], S.tphase[2], tot - S.tphase[0] - S.tphase[1] - S.tphase[2]);
+    fflush(stdout);
   }
   if (S.sol) cusolverDnDestroy(S.sol);
   S.sol = nullptr;
