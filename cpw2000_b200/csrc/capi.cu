@@ -315,13 +315,14 @@ void hk_psi_c16_(const int* mtxd, const int* neig, const double* psi, double* hp
 
 int cpw_b200_ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, double epspsi, int* neig,
                           int mtxds, void* psi, long long ldpsi, void* hpsi, double* ei, const double* hamsm,
-                          int mxdsml, const double* hdiag, int mxdbnd, long long* ihkpsum, void* stream) {
+                          int mxdsml, const double* hdiag, int mxdbnd, long long* ihkpsum, void* stream,
+                          double* itlog, int itlog_rows) {
   if (int s = check_ctx(c)) return s;
   cudaSetDevice(c->device);
   cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
   long long ih = 0;
   int s = ditsp_device(c, ipr, ifail, icmax, iguess, epspsi, neig, mtxds, psi, ldpsi, hpsi, hamsm, mxdsml, hdiag,
-                       mxdbnd, ei, &ih, st);
+                       mxdbnd, ei, &ih, st, itlog, itlog_rows);
   if (ihkpsum) *ihkpsum = ih;
   return s;
 }

@@ -54,7 +54,8 @@ struct DevBuf {
 
 int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, double epspsi, int* neig_io, int mtxds,
                  void* psi, long long ldp, void* hpsi, const double* hamsm, int mxdsml, const double* hdiag,
-                 int mxdbnd, double* ei, long long* ihkpsum, cudaStream_t st);
+                 int mxdbnd, double* ei, long long* ihkpsum, cudaStream_t st, double* itlog = nullptr,
+                 int itlog_rows = 0);
 }  // namespace cpwb
 
 struct cpw_b200_ctx {

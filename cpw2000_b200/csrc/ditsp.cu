@@ -580,7 +580,7 @@ struct Trim {
 // hdiag: host real(mtxd). ei: host real(mxdbnd).
 int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, double epspsi, int* neig_io, int mtxds,
                  void* psi, long long ldp, void* hpsi, const double* hamsm, int mxdsml, const double* hdiag,
-                 int mxdbnd, double* ei, long long* ihkpsum, cudaStream_t st) {
+                 int mxdbnd, double* ei, long long* ihkpsum, cudaStream_t st, double* itlog, int itlog_rows) {
   if (!c->have_basis || !c->have_pot) return fail(kNotReady, "ditsp_c16: basis and potential must be set");
   const int mtxd = c->mtxd;
   int neig = *neig_io;
@@ -1015,6 +1015,15 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
     if (nconv >= ndeg) neig = ndeg;
     xmax = S.xmax_error(neig);
     if (xmax < 0) return fail(kCuda, "ditsp_c16: residual evaluation failed");
+    if (itlog && ic <= itlog_rows) {
+      // iteration log row: elapsed s, xmax, nconv, H|psi> products so far, eg(1:mxdbnd)
+      double* row = itlog + (size_t)(ic - 1) * (4 + mxdbnd);
+      row[0] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+      row[1] = xmax;
+      row[2] = nconv;
+      row[3] = (double)S.ihk;
+      for (int i = 0; i < mxdbnd; ++i) row[4 + i] = i < nsize ? eg[i] : 0.0;
+    }
     if (ipr > 2)
       printf("  ditsp_c16_ritz ic = %d  nconv = %d  niter = %d  nsize = %d  ndeg = %d  xmax = %.6e  e1 = %.12f\n", ic,
              nconv, niter, nsize, ndeg, xmax, eg[0]);

@@ -49,10 +49,13 @@ def ditsp_c16(ipr, icmax, iguess, epspsi, lnewanl, neig, mtxd, mtxds, psi, hpsi,
     return dict(ifail=int(ifail.value), ei=ei[: ne.value].copy(), neig=int(ne.value), lnewanl=bool(lnew.value))
 
 
-def eigensolve(ctx, psi, hpsi, neig, mtxds, hamsm, hdiag, epspsi=1e-5, icmax=40, iguess=0, stream=None, ipr=0):
+def eigensolve(ctx, psi, hpsi, neig, mtxds, hamsm, hdiag, epspsi=1e-5, icmax=40, iguess=0, stream=None, ipr=0,
+               trace=False):
     """ditsp on device-resident column-major complex128 psi/hpsi (mxdbnd = psi.shape[1] columns).
 
-    Returns dict(ifail, ei, neig, ihkpsum, converged).
+    Returns dict(ifail, ei, neig, ihkpsum, converged[, trace]). With trace=True,
+    ``trace`` is an (iterations, 4 + mxdbnd) array: elapsed s, xmax, nconv,
+    H|psi> products and the Ritz values after every outer iteration.
     """
     L = _lib.lib()
     mxdbnd = int(psi.shape[1])
@@ -63,11 +66,16 @@ def eigensolve(ctx, psi, hpsi, neig, mtxds, hamsm, hdiag, epspsi=1e-5, icmax=40,
     ne = C.c_int(int(neig))
     ih = C.c_longlong(0)
     s = stream if stream is not None else torch_stream_handle(psi.device)
+    log = np.zeros((int(icmax), 4 + mxdbnd)) if trace else None
     st = L.cpw_b200_ditsp_device(ctx.handle, int(ipr), C.byref(ifail), int(icmax), int(iguess), float(epspsi), C.byref(ne),
                                  int(mtxds), C.c_void_p(psi.data_ptr()), ctx._ld(psi), C.c_void_p(hpsi.data_ptr()),
                                  dptr(ei), zptr(hamsm), int(hamsm.shape[0]), dptr(hdiag), mxdbnd, C.byref(ih),
-                                 C.c_void_p(s))
+                                 C.c_void_p(s), dptr(log) if trace else None, int(icmax) if trace else 0)
     if st not in (0, NOT_CONVERGED):
         raise CpwB200Error(st, L.cpw_b200_last_error().decode(errors="replace"))
-    return dict(ifail=int(ifail.value), ei=ei[: ne.value].copy(), neig=int(ne.value), ihkpsum=int(ih.value),
-                converged=st == 0)
+    out = dict(ifail=int(ifail.value), ei=ei[: ne.value].copy(), neig=int(ne.value), ihkpsum=int(ih.value),
+               converged=st == 0)
+    if trace:
+        used = int(np.count_nonzero(log[:, 0] > 0))
+        out["trace"] = log[:used]
+    return out

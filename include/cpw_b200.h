@@ -126,10 +126,14 @@ void hk_psi_nl_c16_(const int* mtxd, const int* neig, const double* psi, double*
  * host output (mxdbnd). *neig may grow to the degeneracy-closed count. Returns
  * CPW_B200_NOT_CONVERGED with *ifail = number of accurate digits when epspsi is
  * not reached in icmax outer iterations. ihkpsum (may be NULL) receives the
- * number of H|psi> band applications. Synchronous. */
+ * number of H|psi> band applications. Synchronous. itlog (may be NULL) is a host
+ * array of itlog_rows rows of (4 + mxdbnd) doubles; after outer iteration ic
+ * row ic-1 holds the elapsed seconds, xmax, nconv, the H|psi> products so far
+ * and the current Ritz values (the time-to-eigenvalue trace). */
 int cpw_b200_ditsp_device(cpw_b200_ctx* ctx, int ipr, int* ifail, int icmax, int iguess, double epspsi, int* neig,
                           int mtxds, void* psi, long long ldpsi, void* hpsi, double* ei, const double* hamsm,
-                          int mxdsml, const double* hdiag, int mxdbnd, long long* ihkpsum, void* stream);
+                          int mxdsml, const double* hdiag, int mxdbnd, long long* ihkpsum, void* stream,
+                          double* itlog, int itlog_rows);
 
 /* Src/ditsp/ditsp_c16.f90:20-27 with host arrays (psi, hpsi complex(8) (mxddim, mxdbnd)). */
 int cpw_b200_ditsp_c16(const int* ipr, int* ifail, const int* icmax, const int* iguess, const double* epspsi,
