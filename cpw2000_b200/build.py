@@ -62,7 +62,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
                     print(f"compiled {name}", err, file=sys.stderr)
     objs = [BUILD / (s.stem + ".o") for s in sources()]
     if jobs or not OUT.exists() or OUT.stat().st_mtime < max(o.stat().st_mtime for o in objs):
-        cmd = [exe, *ARCH, "-shared", "-o", str(OUT), *map(str, objs), "-lcublas", "-lcusolver", "-lcudart"]
+        cmd = [exe, *ARCH, "-shared", "-o", str(OUT), *map(str, objs), "-lcublas", "-lcusolver", "-lcufft", "-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")

@@ -380,6 +380,28 @@ void ditsp_c16_(const int* ipr, int* ifail, const int* icmax, const int* iguess,
   if (s != 0 && s != CPW_B200_NOT_CONVERGED) stop_like_fortran("ditsp_c16");
 }
 
+int cpw_b200_density_device(cpw_b200_ctx* c, int neig, const void* psi, long long ldpsi, const double* occ,
+                            void* rho, void* stream) {
+  if (int s = check_ctx(c)) return s;
+  cudaSetDevice(c->device);
+  return density_device(c, neig, psi, ldpsi, occ, rho, stream ? (cudaStream_t)stream : c->stream);
+}
+
+int cpw_b200_structure_grad_device(cpw_b200_ctx* c, const void* g, int natom, const int* atom_type, const double* tau,
+                                   int ntype, const void* vgt, double* dedtau, void* stream) {
+  if (int s = check_ctx(c)) return s;
+  cudaSetDevice(c->device);
+  return structure_grad_device(c, g, natom, atom_type, tau, ntype, vgt, dedtau,
+                               stream ? (cudaStream_t)stream : c->stream);
+}
+
+int cpw_b200_nl_grad_device(cpw_b200_ctx* c, int neig, const void* psi, long long ldpsi, const double* occ,
+                            const int* proj_atom, int natom, double* dedtau, void* stream) {
+  if (int s = check_ctx(c)) return s;
+  cudaSetDevice(c->device);
+  return nl_grad_device(c, neig, psi, ldpsi, occ, proj_atom, natom, dedtau, stream ? (cudaStream_t)stream : c->stream);
+}
+
 int cpw_b200_hk_psi_nl_c16(const int* mtxd, const int* neig, const double* psi, double* hpsi, const double* anlga,
                            const double* xnlkb, const int* nanl, const int* ladd, const int* mxddim,
                            const int* mxdbnd, const int* mxdanl) {

@@ -166,6 +166,7 @@ int ctx_set_basis(cpw_b200_ctx* c, int mtxd, const int* isort, const int* kgv, i
     if ((s = upload(c->pw_idx, idx.data(), idx.size() * sizeof(int)))) return s;
     if ((s = upload(c->pw_pos, pos.data(), pos.size() * sizeof(int)))) return s;
     if ((s = upload(c->ekpg, ekpg, (size_t)mtxd * sizeof(double)))) return s;
+    if ((s = upload(c->kgvb, g.data(), g.size() * sizeof(int)))) return s;
   }
   const int ns[3] = {n1, n2, n3};
   for (int d = 0; d < 3; ++d) {
@@ -253,6 +254,9 @@ int ctx_set_projectors(cpw_b200_ctx* c, int nanl, const double* anlga, int ld, c
   }
   k_scale_cols<<<1184, 256, 0, c->stream>>>((const C2<double>*)c->anl.p, (C2<double>*)c->anld.p,
                                             (const double*)dx.p, m, nanl, m, m);
+  c->xnl_h.resize(nanl);
+  e = cudaMemcpyAsync(c->xnl_h.data(), dx.p, nanl * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "set_projectors copy");
   e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "set_projectors");
   return kOk;

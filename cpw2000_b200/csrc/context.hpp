@@ -56,6 +56,12 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
                  void* psi, long long ldp, void* hpsi, const double* hamsm, int mxdsml, const double* hdiag,
                  int mxdbnd, double* ei, long long* ihkpsum, cudaStream_t st, double* itlog = nullptr,
                  int itlog_rows = 0);
+int density_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, const double* occ, void* rho,
+                   cudaStream_t st);
+int structure_grad_device(cpw_b200_ctx* c, const void* g, int natom, const int* atom_type, const double* tau,
+                          int ntype, const void* vgt, double* dedtau, cudaStream_t st);
+int nl_grad_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, const double* occ,
+                   const int* proj_atom, int natom, double* dedtau, cudaStream_t st);
 }  // namespace cpwb
 
 struct cpw_b200_ctx {
@@ -70,7 +76,7 @@ struct cpw_b200_ctx {
   int mtxd = 0;
   int ident = 0;                // leading dimension id of the reference box (kmscr(7))
   cpwb::LocalPlan plan{};
-  cpwb::DevBuf plane_start, pw_idx, pw_pos, ekpg;
+  cpwb::DevBuf plane_start, pw_idx, pw_pos, ekpg, kgvb;   // kgvb: (3, mtxd) G of the basis
   cpwb::DevBuf tw64[3], tw32[3];
 
   // local potential on the box, [z][y][x] scaled by 1/N
@@ -81,6 +87,7 @@ struct cpw_b200_ctx {
   // KB projectors (column-major mtxd x nanl) pre-multiplied by xnlkb in anld
   int nanl = 0;
   cpwb::DevBuf anl, anld, proj;
+  std::vector<double> xnl_h;    // host copy of xnlkb
 
   cpwb::StageTimer timer;
 

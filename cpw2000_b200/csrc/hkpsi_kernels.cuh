@@ -364,7 +364,24 @@ cudaError_t launch_impl(const LocalPlan& p, int nbc, int band0, const C2<double>
   return cudaGetLastError();
 }
 
+// Launch kernel A alone (scatter + inverse x + inverse y into the slab W).
+template <typename T, int RX1, int RX2, int RY1, int RY2, int TC>
+cudaError_t launch_inv_impl(const LocalPlan& p, int nbc, int band0, const C2<double>* psi, long long ldpsi,
+                            const int* plane_start, const int* pw_idx, const int* pw_pos, const C2<T>* twx,
+                            const C2<T>* twy, C2<T>* W, cudaStream_t st) {
+  const size_t sm_pl = smem_planes<T>(p);
+  auto* ka = k_inv_xy<T, RX1, RX2, RY1, RY2, TC>;
+  cudaError_t e = cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pl);
+  if (e != cudaSuccess) return e;
+  ka<<<dim3(p.nz, nbc), kThreadsPlanes, sm_pl, st>>>(p, band0, psi, ldpsi, plane_start, pw_idx, pw_pos, twx, twy, W);
+  return cudaGetLastError();
+}
+
 }  // namespace kern
+
+#define CPWB_INV_ARGS(T)                                                                                     \
+  const LocalPlan &p, int nbc, int band0, const C2<double>*psi, long long ldpsi, const int *plane_start,     \
+      const int *pw_idx, const int *pw_pos, const C2<T>*twx, const C2<T>*twy, C2<T>*W, cudaStream_t st
 
 #define CPWB_LAUNCH_ARGS(T)                                                                                  \
   const LocalPlan &p, int nbc, int band0, const C2<double>*psi, long long ldpsi, C2<double>*hpsi,            \
@@ -372,7 +389,8 @@ cudaError_t launch_impl(const LocalPlan& p, int nbc, int band0, const C2<double>
       const T *vr, const C2<T>*twx, const C2<T>*twy, const C2<T>*twz, C2<T>*W, cudaStream_t st,             \
       cudaEvent_t *ev
 
-#define CPWB_INSTANTIATE(T, RX1, RX2, RY1, RY2, RZ1, RZ2, TC, CB) \
-  template cudaError_t kern::launch_impl<T, RX1, RX2, RY1, RY2, RZ1, RZ2, TC, CB>(CPWB_LAUNCH_ARGS(T));
+#define CPWB_INSTANTIATE(T, RX1, RX2, RY1, RY2, RZ1, RZ2, TC, CB)                                        \
+  template cudaError_t kern::launch_impl<T, RX1, RX2, RY1, RY2, RZ1, RZ2, TC, CB>(CPWB_LAUNCH_ARGS(T)); \
+  template cudaError_t kern::launch_inv_impl<T, RX1, RX2, RY1, RY2, TC>(CPWB_INV_ARGS(T));
 
 }  // namespace cpwb

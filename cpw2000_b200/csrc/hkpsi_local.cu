@@ -7,8 +7,9 @@ namespace cpwb {
 
 namespace kern {
 // specialisations compiled in hkpsi_spec_*.cu
-#define CPWB_DECLARE(T, RX1, RX2, RY1, RY2, RZ1, RZ2, TC, CB) \
-  extern template cudaError_t launch_impl<T, RX1, RX2, RY1, RY2, RZ1, RZ2, TC, CB>(CPWB_LAUNCH_ARGS(T));
+#define CPWB_DECLARE(T, RX1, RX2, RY1, RY2, RZ1, RZ2, TC, CB)                                                  \
+  extern template cudaError_t launch_impl<T, RX1, RX2, RY1, RY2, RZ1, RZ2, TC, CB>(CPWB_LAUNCH_ARGS(T));        \
+  extern template cudaError_t launch_inv_impl<T, RX1, RX2, RY1, RY2, TC>(CPWB_INV_ARGS(T));
 CPWB_DECLARE(double, 4, 8, 4, 8, 4, 8, 32, 32)
 CPWB_DECLARE(float, 4, 8, 4, 8, 4, 8, 32, 32)
 CPWB_DECLARE(double, 5, 8, 5, 8, 5, 8, 32, 32)
@@ -44,5 +45,26 @@ cudaError_t launch_local(CPWB_LAUNCH_ARGS(T)) {
 
 template cudaError_t launch_local<double>(CPWB_LAUNCH_ARGS(double));
 template cudaError_t launch_local<float>(CPWB_LAUNCH_ARGS(float));
+
+template <typename T>
+cudaError_t launch_inverse_xy(CPWB_INV_ARGS(T)) {
+  const bool cubic = p.n1 == p.n2 && p.n2 == p.n3 && p.tcol == 32 && p.cb == 32;
+  if (cubic && is_split(p.dx, 8, 12))
+    return kern::launch_inv_impl<T, 8, 12, 8, 12, 32>(p, nbc, band0, psi, ldpsi, plane_start, pw_idx, pw_pos, twx,
+                                                     twy, W, st);
+  if (cubic && is_split(p.dx, 12, 12))
+    return kern::launch_inv_impl<T, 12, 12, 12, 12, 32>(p, nbc, band0, psi, ldpsi, plane_start, pw_idx, pw_pos, twx,
+                                                       twy, W, st);
+  if (cubic && is_split(p.dx, 4, 8))
+    return kern::launch_inv_impl<T, 4, 8, 4, 8, 32>(p, nbc, band0, psi, ldpsi, plane_start, pw_idx, pw_pos, twx, twy,
+                                                   W, st);
+  if (cubic && is_split(p.dx, 5, 8))
+    return kern::launch_inv_impl<T, 5, 8, 5, 8, 32>(p, nbc, band0, psi, ldpsi, plane_start, pw_idx, pw_pos, twx, twy,
+                                                   W, st);
+  return kern::launch_inv_impl<T, 0, 0, 0, 0, 0>(p, nbc, band0, psi, ldpsi, plane_start, pw_idx, pw_pos, twx, twy, W,
+                                                st);
+}
+template cudaError_t launch_inverse_xy<double>(CPWB_INV_ARGS(double));
+template cudaError_t launch_inverse_xy<float>(CPWB_INV_ARGS(float));
 
 }  // namespace cpwb

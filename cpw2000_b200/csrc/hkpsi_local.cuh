@@ -65,4 +65,11 @@ cudaError_t launch_local(const LocalPlan& p, int nbc, int band0, const C2<double
                          const C2<T>* twy, const C2<T>* twz, C2<T>* W, cudaStream_t st,
                          cudaEvent_t* ev = nullptr);
 
+// Kernel A alone for bands [band0, band0+nbc): the kept z-planes of every band,
+// inverse-transformed in x and y, into W (density / adjoint path).
+template <typename T>
+cudaError_t launch_inverse_xy(const LocalPlan& p, int nbc, int band0, const C2<double>* psi, long long ldpsi,
+                              const int* plane_start, const int* pw_idx, const int* pw_pos, const C2<T>* twx,
+                              const C2<T>* twy, C2<T>* W, cudaStream_t st);
+
 }  // namespace cpwb

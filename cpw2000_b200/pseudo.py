@@ -224,6 +224,42 @@ def local_potential_box(species, adot, box, idpad: int = 0):
     return box_arr.reshape(-1), veffr1
 
 
+def local_form_factors_box(species, adot, box):
+    """Form factors v_t(G) of every species on the box, FFT order, shape (ntype, n3, n2, n1).
+
+    The same coefficients local_potential_box places (Nyquist planes zero), so
+    that V(G) = sum_a e^{-2 pi i m.tau_a} v_t(G) reproduces vscr.
+    """
+    n1, n2, n3 = box
+    vcell, bdot = adot_to_bdot(adot)
+    mz, my, mx = np.meshgrid(*[np.fft.fftfreq(n, 1.0 / n) for n in (n3, n2, n1)], indexing="ij")
+    mm = np.stack([mx.ravel(), my.ravel(), mz.ravel()])
+    g2 = np.einsum("in,ij,jn->n", mm, bdot, mm).reshape(n3, n2, n1)
+    out = np.zeros((len(species), n3, n2, n1))
+    for t, sp in enumerate(species):
+        out[t] = -sp.v0 * (2 * PI * sp.sigma ** 2) ** 1.5 * np.exp(-0.5 * g2 * sp.sigma ** 2) / vcell
+    for ax, n in ((3, n1), (2, n2), (1, n3)):
+        if n % 2 == 0:
+            sl = [slice(None)] * 4
+            sl[ax] = n // 2
+            out[tuple(sl)] = 0.0
+    return out
+
+
+def proj_atom_map(species, nkb):
+    """0-based global atom index of each projector column (order type -> l -> m -> atom)."""
+    out = []
+    off = 0
+    for t, sp in enumerate(species):
+        for l in range(4):
+            if nkb[t, l] == 0:
+                continue
+            for _m in range(2 * l + 1):
+                out.extend(range(off, off + sp.natom))
+        off += sp.natom
+    return np.array(out, dtype=np.int32)
+
+
 def potential_fourier(vscr, box, ident):
     """Fourier coefficients Vt(m) = (1/N) sum_r vscr(r) e^{-i 2pi m.r/n} on the box."""
     n1, n2, n3 = box

@@ -95,6 +95,25 @@ int cpw_b200_hk_psi_device(cpw_b200_ctx* ctx, int neig, const void* psi, long lo
 int cpw_b200_hk_psi_loc_device(cpw_b200_ctx* ctx, int neig, const void* psi, long long ldpsi, void* hpsi,
                                long long ldhpsi, void* stream);
 
+/* ---- adjoint of H|psi> for fixed wavefunctions (Hellmann-Feynman) ----
+ * For E = sum_n occ_n <psi_n|H|psi_n>:
+ * density: rho(r) = sum_n occ_n |psi_n(r)|^2 on the box, device doubles laid out
+ *   [z][y][x] (n1*n2*n3), psi_n(r) the unscaled backward transform, as the mesh
+ *   density of Src/omp/charge_by_fft.f90:185-199; dE/dvscr(r) = rho(r)/(n1 n2 n3).
+ * structure_grad: dE/dtau (host natom x 3, lattice coordinates) of sum_r g(r) V(r)
+ *   for V(G) = sum_a e^{-2 pi i G.tau_a} v_t(G): g device [z][y][x] box doubles,
+ *   vgt device ntype x n1 x n2 x n3 form factors v_t(G) in FFT order, tau host
+ *   natom x 3, atom_type host 0-based (local term of Src/ALFA/for_str_local_force.f90).
+ * nl_grad: dE/dtau of the Kleinman-Bylander energy for the context's projectors;
+ *   proj_atom (host, nanl) is the 0-based atom of each projector column (the KB
+ *   term of Src/ALFA/for_str_nl_kb.f90). Forces are minus these derivatives. */
+int cpw_b200_density_device(cpw_b200_ctx* ctx, int neig, const void* psi, long long ldpsi, const double* occ,
+                            void* rho, void* stream);
+int cpw_b200_structure_grad_device(cpw_b200_ctx* ctx, const void* g, int natom, const int* atom_type,
+                                   const double* tau, int ntype, const void* vgt, double* dedtau, void* stream);
+int cpw_b200_nl_grad_device(cpw_b200_ctx* ctx, int neig, const void* psi, long long ldpsi, const double* occ,
+                            const int* proj_atom, int natom, double* dedtau, void* stream);
+
 /* ---- drop-ins with the reference argument lists ---- */
 
 /* Src/hk_psi/reference/hk_psi_c16.f90:28-32. lnewanl != 0 tells the library
