@@ -6,6 +6,8 @@
 // compile-time forms get constant index arithmetic and register allocation
 // sized for their own radices; the all-zero form serves any supported box.
 #pragma once
+#include <algorithm>
+
 #include "hkpsi_local.cuh"
 
 namespace cpwb {
@@ -215,6 +217,139 @@ k_z_vloc(LocalPlan p, const T* __restrict__ vr, const C2<T>* __restrict__ twz, C
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// B (pipelined): one CTA per (CB xy-columns, band group). The V(r)/N tile of
+// the columns is loaded into shared memory once; the kept planes of band b+1
+// stream in with cp.async while band b is transformed, so global latency
+// overlaps the butterflies. Same arithmetic as k_z_vloc.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async_bytes(void* smem, const void* gmem, int bytes) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  if (bytes == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+  else if (bytes == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// shared memory of k_z_vloc_pipe: work columns, two staging buffers of kept planes, twiddles, V tile
+template <typename T> inline size_t smem_columns_pipe(const LocalPlan& p, int cb) {
+  return sizeof(C2<T>) * ((size_t)p.n3 * cb + 2 * (size_t)p.nz * cb + p.n3) + sizeof(T) * (size_t)p.n3 * cb;
+}
+
+template <typename T, int RZ1, int RZ2, int CB>
+__global__ void __launch_bounds__(kThreadsCols, 1)
+k_z_vloc_pipe(LocalPlan p, int nbc, int bands_per_group, const T* __restrict__ vr, const C2<T>* __restrict__ twz,
+              C2<T>* __restrict__ W) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int cb = CB ? CB : p.cb;
+  const int r1 = RZ1 ? RZ1 : p.dz.r1, r2 = RZ2 ? RZ2 : p.dz.r2;
+  const int n3 = RZ1 ? RZ1 * RZ2 : p.n3;
+  const int nz = p.nz;
+  C2<T>* Cs = reinterpret_cast<C2<T>*>(smem_raw);
+  C2<T>* Ws = Cs + (size_t)n3 * cb;
+  C2<T>* sz = Ws + 2 * (size_t)nz * cb;
+  T* Vs = reinterpret_cast<T*>(sz + n3);
+  const long long c0 = (long long)blockIdx.x * cb;
+  const int ncol = (int)min((long long)cb, p.plane - c0);
+  const int b_lo = blockIdx.y * bands_per_group;
+  const int b_hi = min(nbc, b_lo + bands_per_group);
+  if (b_lo >= b_hi) return;
+  const int tid = threadIdx.x, nt = blockDim.x;
+
+  auto stage = [&](int b, int buf) {
+    const C2<T>* Wb = W + (size_t)b * nz * (size_t)p.plane + c0;
+    C2<T>* dst = Ws + (size_t)buf * nz * cb;
+    for (int it = tid; it < cb * nz; it += nt) {
+      const int cl = it % cb, zi = it / cb;
+      if (cl < ncol) cp_async_bytes(dst + (size_t)zi * cb + cl, Wb + (size_t)zi * p.plane + cl, (int)sizeof(C2<T>));
+    }
+  };
+  for (int i = tid; i < n3; i += nt) sz[i] = twz[i];
+  for (int it = tid; it < cb * n3; it += nt) {
+    const int cl = it % cb, z = it / cb;
+    if (cl < ncol) cp_async_bytes(Vs + (size_t)z * cb + cl, vr + (size_t)z * p.plane + c0 + cl, (int)sizeof(T));
+  }
+  stage(b_lo, 0);
+  cp_async_commit();
+  if (b_lo + 1 < b_hi) stage(b_lo + 1, 1);
+  cp_async_commit();
+
+  for (int b = b_lo; b < b_hi; ++b) {
+    const int buf = (b - b_lo) & 1;
+    cp_async_wait<1>();       // every group but the newest (band b+1) has landed
+    __syncthreads();
+    const C2<T>* Wsb = Ws + (size_t)buf * nz * cb;
+    // inverse pass 1 straight from the staged kept planes
+    for (int it = tid; it < cb * r2; it += nt) {
+      const int cl = it % cb, n2i = it / cb;
+      if (cl < ncol) {
+        with_radix<RZ1>(r1, [&](auto rc_) {
+          constexpr int RR = decltype(rc_)::value;
+          C2<T> v[RR];
+#pragma unroll
+          for (int a = 0; a < RR; ++a) {
+            const int zi = idx_to_kept(r2 * a + n2i, p.kd3, n3, nz);
+            v[a] = zi >= 0 ? Wsb[(size_t)zi * cb + cl] : czero<T>();
+          }
+          DFT<RR, +1, T>::run(v);
+#pragma unroll
+          for (int a = 0; a < RR; ++a)
+            Cs[(size_t)(r2 * a + n2i) * cb + cl] = a == 0 ? v[0] : cmulc<T>(v[a], sz[n2i * a]);
+        });
+      }
+    }
+    __syncthreads();
+    // the staging buffer of band b is free: prefetch band b+2 into it
+    if (b + 2 < b_hi) stage(b + 2, buf);
+    cp_async_commit();
+    // inverse pass 2 -> V/N -> forward pass 1, in registers
+    for (int it = tid; it < cb * r1; it += nt) {
+      const int cl = it % cb, k1 = it / cb;
+      if (cl < ncol) {
+        with_radix<RZ2>(r2, [&](auto rc_) {
+          constexpr int RR = decltype(rc_)::value;
+          C2<T> v[RR];
+#pragma unroll
+          for (int a = 0; a < RR; ++a) v[a] = Cs[(size_t)(r2 * k1 + a) * cb + cl];
+          DFT<RR, +1, T>::run(v);
+#pragma unroll
+          for (int a = 0; a < RR; ++a) v[a] = scal<T>(v[a], Vs[(size_t)(k1 + r1 * a) * cb + cl]);
+          DFT<RR, -1, T>::run(v);
+#pragma unroll
+          for (int a = 0; a < RR; ++a)
+            Cs[(size_t)(r2 * k1 + a) * cb + cl] = a == 0 ? v[0] : cmul<T>(v[a], sz[k1 * a]);
+        });
+      }
+    }
+    __syncthreads();
+    // forward pass 2, kept planes back to the slab
+    C2<T>* Wb = W + (size_t)b * nz * (size_t)p.plane + c0;
+    for (int it = tid; it < cb * r2; it += nt) {
+      const int cl = it % cb, m2 = it / cb;
+      if (cl < ncol) {
+        with_radix<RZ1>(r1, [&](auto rc_) {
+          constexpr int RR = decltype(rc_)::value;
+          C2<T> v[RR];
+#pragma unroll
+          for (int a = 0; a < RR; ++a) v[a] = Cs[(size_t)(r2 * a + m2) * cb + cl];
+          DFT<RR, -1, T>::run(v);
+#pragma unroll
+          for (int a = 0; a < RR; ++a) {
+            const int zi = idx_to_kept(m2 + r2 * a, p.kd3, n3, nz);
+            if (zi >= 0) Wb[(size_t)zi * p.plane + cl] = v[a];
+          }
+        });
+      }
+    }
+  }
+  cp_async_wait<0>();
+}
+
 // ---------------------------------------------------------------------------
 // C: forward y + forward x + gather + kinetic, one CTA per (band, kept z-plane)
 // ---------------------------------------------------------------------------
@@ -343,20 +478,37 @@ cudaError_t launch_impl(const LocalPlan& p, int nbc, int band0, const C2<double>
                         const int* pw_pos, const double* ekpg, const T* vr, const C2<T>* twx, const C2<T>* twy,
                         const C2<T>* twz, C2<T>* W, cudaStream_t st, cudaEvent_t* ev) {
   const size_t sm_pl = smem_planes<T>(p);
-  const size_t sm_co = smem_columns<T>(p);
   auto* ka = k_inv_xy<T, RX1, RX2, RY1, RY2, TC>;
-  auto* kb = k_z_vloc<T, RZ1, RZ2, CB>;
   auto* kc = k_fwd_xy<T, RX1, RX2, RY1, RY2, TC>;
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pl)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pl)) != cudaSuccess) return e;
-  if ((e = cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_co)) != cudaSuccess) return e;
+  int nsm = 148, dev = 0, smax = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   dim3 gA(p.nz, nbc);
   if (ev) cudaEventRecord(ev[0], st);
   ka<<<gA, kThreadsPlanes, sm_pl, st>>>(p, band0, psi, ldpsi, plane_start, pw_idx, pw_pos, twx, twy, W);
   if (ev) cudaEventRecord(ev[1], st);
-  dim3 gB((unsigned)((p.plane + p.cb - 1) / p.cb), nbc);
-  kb<<<gB, kThreadsCols, sm_co, st>>>(p, vr, twz, W);
+  const size_t sm_pipe = smem_columns_pipe<T>(p, p.cb);
+  const long long tiles = (p.plane + p.cb - 1) / p.cb;
+  if (sm_pipe > (size_t)smax) {
+    // the staged form does not fit: one CTA per (band, column tile)
+    const size_t sm_co = smem_columns<T>(p);
+    auto* kb = k_z_vloc<T, RZ1, RZ2, CB>;
+    if ((e = cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_co)) != cudaSuccess) return e;
+    kb<<<dim3((unsigned)tiles, nbc), kThreadsCols, sm_co, st>>>(p, vr, twz, W);
+  } else {
+    // column tiles x band groups: enough CTAs for two per SM on small boxes
+    long long groups = std::max(1LL, std::min((long long)nbc, (2LL * nsm + tiles - 1) / tiles));
+    const int per = (int)((nbc + groups - 1) / groups);
+    groups = (nbc + per - 1) / per;
+    auto* kbp = k_z_vloc_pipe<T, RZ1, RZ2, CB>;
+    if ((e = cudaFuncSetAttribute(kbp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pipe)) != cudaSuccess)
+      return e;
+    kbp<<<dim3((unsigned)tiles, (unsigned)groups), kThreadsCols, sm_pipe, st>>>(p, nbc, per, vr, twz, W);
+  }
   if (ev) cudaEventRecord(ev[2], st);
   kc<<<gA, kThreadsPlanes, sm_pl, st>>>(p, band0, psi, ldpsi, hpsi, ldh, plane_start, pw_idx, pw_pos, ekpg, twx,
                                         twy, W);
