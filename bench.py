@@ -382,7 +382,7 @@ def run_profile(args, local):
     nb = args.bands
     psi = torch.from_numpy(np.ascontiguousarray(configs.random_psi(d["mtxd"], nb, 5).T)).to(dev).t()
     hpsi = torch.empty((nb, d["mtxd"]), dtype=torch.complex128, device=dev).t()
-    ctx = H.Context(local, precision=H.MIXED if args.precision == "mixed" else H.FP64).setup(d)
+    ctx = H.Context(local, precision={"fp64": H.FP64, "mixed": H.MIXED, "mixed_tc": H.MIXED_TC}[args.precision]).setup(d)
     ctx.set_slab_budget(4 << 30)
     for _ in range(args.warmup + args.steps):
         ctx.hk_psi(psi, hpsi)
@@ -394,7 +394,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--mode", choices=["bench", "profile"], default="bench")
     ap.add_argument("--bands", type=int, default=NB, help="profile mode: bands per call")
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64", help="profile mode precision")
+    ap.add_argument("--precision", choices=["fp64", "mixed", "mixed_tc"], default="fp64", help="profile mode precision")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)

@@ -169,14 +169,17 @@ void* cpw_b200_stream(cpw_b200_ctx* c) { return c ? (void*)c->stream : nullptr; 
 
 int cpw_b200_synchronize(cpw_b200_ctx* c) {
   if (int s = check_ctx(c)) return s;
-  cudaError_t e = cudaStreamSynchronize(c->stream);
-  return e == cudaSuccess ? kOk : cuda_fail(e, "synchronize");
+  cudaSetDevice(c->device);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_fail(e, "synchronize");
+  return tc_check_error(c);   // a bounded device wait that gave up reports CPW_B200_TIMEOUT
 }
 
 int cpw_b200_set_precision(cpw_b200_ctx* c, int mode) {
   if (int s = check_ctx(c)) return s;
-  if (mode != CPW_B200_FP64 && mode != CPW_B200_MIXED) return fail(kBadArg, "set_precision: unknown mode");
-  if (mode != c->precision && c->have_basis) {
+  if (mode != CPW_B200_FP64 && mode != CPW_B200_MIXED && mode != CPW_B200_MIXED_TC)
+    return fail(kBadArg, "set_precision: unknown mode");
+  if ((mode != 0) != (c->precision != 0) && c->have_basis) {
     // shared-memory tiling depends on the element size: caller must set the k-point again
     c->have_basis = false;
     c->have_pot = false;

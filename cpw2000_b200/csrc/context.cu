@@ -257,8 +257,10 @@ int ctx_set_projectors(cpw_b200_ctx* c, int nanl, const double* anlga, int ld, c
   c->xnl_h.resize(nanl);
   e = cudaMemcpyAsync(c->xnl_h.data(), dx.p, nanl * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "set_projectors copy");
+  c->tc_ready = false;
   e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "set_projectors");
+  if (c->precision == 2) return tc_prepare_projectors(c);
   return kOk;
 }
 
@@ -316,6 +318,13 @@ int ctx_hkpsi_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, 
     cublasStatus_t bs;
     cudaEvent_t t0 = c->timer.on ? c->timer.take() : nullptr, t1 = c->timer.on ? c->timer.take() : nullptr;
     cudaEvent_t t2 = c->timer.on ? c->timer.take() : nullptr;
+    if (c->precision == 2 && c->tc_ready) {
+      // opt-in mixed form: split-TF32 tensor-core products (nl_tc.cu)
+      if ((s = tc_nl_apply(c, nb, psi, ldpsi, hpsi, ldh, st, t0, t1, t2))) return s;
+      c->timer.mark(kStNlProj, t0, t1);
+      c->timer.mark(kStNlExpand, t1, t2);
+      return kOk;
+    }
     if (t0) cudaEventRecord(t0, st);
     // P = X^H psi (hk_psi_nl_c16.f90:82); hpsi += (X D) P (:87-96)
     bs = cublasZgemm(c->blas, CUBLAS_OP_C, CUBLAS_OP_N, c->nanl, nb, c->mtxd, &one, (const cuDoubleComplex*)c->anl.p,

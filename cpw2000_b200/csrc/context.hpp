@@ -56,6 +56,10 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
                  void* psi, long long ldp, void* hpsi, const double* hamsm, int mxdsml, const double* hdiag,
                  int mxdbnd, double* ei, long long* ihkpsum, cudaStream_t st, double* itlog = nullptr,
                  int itlog_rows = 0);
+int tc_prepare_projectors(cpw_b200_ctx* c);
+int tc_nl_apply(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh, cudaStream_t st,
+                cudaEvent_t t0, cudaEvent_t t1, cudaEvent_t t2);
+int tc_check_error(cpw_b200_ctx* c);
 int density_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, const double* occ, void* rho,
                    cudaStream_t st);
 int structure_grad_device(cpw_b200_ctx* c, const void* g, int natom, const int* atom_type, const double* tau,
@@ -68,7 +72,7 @@ struct cpw_b200_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   cublasHandle_t blas = nullptr;
-  int precision = 0;            // 0: FP64 local + FP64 projector GEMMs; 1: FP32 local (mixed)
+  int precision = 0;            // 0: FP64; 1: FP32 local + FP64 projector GEMMs; 2: 1 with split-TF32 tensor-core projectors
   size_t slab_budget = 512ull << 20;
 
   // basis of the current k-point
@@ -88,6 +92,10 @@ struct cpw_b200_ctx {
   int nanl = 0;
   cpwb::DevBuf anl, anld, proj;
   std::vector<double> xnl_h;    // host copy of xnlkb
+  // mixed precision: split-TF32 operands of the tensor-core projector GEMMs
+  cpwb::DevBuf tc_a1, tc_a2, tc_part, tc_b2, tc_err;
+  long long tc_k1p = 0, tc_k2p = 0;
+  bool tc_ready = false;
 
   cpwb::StageTimer timer;
 

@@ -19,6 +19,7 @@ from ._lib import check, dptr, iptr, zptr
 
 FP64 = 0
 MIXED = 1
+MIXED_TC = 2
 
 
 def _as_f(a, dtype):
@@ -106,6 +107,10 @@ class Context:
 
     def set_precision(self, mode: int):
         check(self._L.cpw_b200_set_precision(self.handle, int(mode)))
+
+    def synchronize(self):
+        """Wait for the device; raises if a bounded device-side wait gave up."""
+        check(self._L.cpw_b200_synchronize(self.handle))
 
     def set_slab_budget(self, nbytes: int):
         check(self._L.cpw_b200_set_slab_budget(self.handle, int(nbytes)))

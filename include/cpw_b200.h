@@ -46,7 +46,11 @@ extern "C" {
 
 /* ---- precision modes ---- */
 #define CPW_B200_FP64 0  /* plain FP64 everywhere (the drop-in default) */
-#define CPW_B200_MIXED 1 /* FP32 FFT/V_loc; projector GEMMs and subspace steps per the mixed form */
+#define CPW_B200_MIXED 1 /* FP32 FFT/V_loc, FP64 projector GEMMs, FP64 subspace steps */
+/* MIXED with the projector products as split-TF32 (hi.hi + hi.lo + lo.hi) tcgen05 GEMMs with FP32
+ * accumulation in tensor memory: ~1e-6 relative error in the projector term; opt-in, set before the
+ * projectors (they are prepared in the split layouts at set_projectors). */
+#define CPW_B200_MIXED_TC 2
 
 typedef struct cpw_b200_ctx cpw_b200_ctx;
 
@@ -60,6 +64,8 @@ int cpw_b200_create(cpw_b200_ctx** ctx, int device);
 int cpw_b200_destroy(cpw_b200_ctx* ctx);
 /* The context's own CUDA stream (cudaStream_t as void*). */
 void* cpw_b200_stream(cpw_b200_ctx* ctx);
+/* Waits for all work on the device; returns CPW_B200_TIMEOUT if a bounded
+ * device-side wait of an earlier kernel gave up (its outputs are then invalid). */
 int cpw_b200_synchronize(cpw_b200_ctx* ctx);
 int cpw_b200_set_precision(cpw_b200_ctx* ctx, int mode);
 /* Device bytes the FFT slab of one band chunk may use (default 512 MiB). */

@@ -187,3 +187,27 @@ def test_unsupported_box_is_rejected(cuda):
     with pytest.raises(CpwB200Error) as e:
         ctx.set_kpoint(d["mtxd"], d["isort"], d["kgv"], d["ekpg"], km)
     assert e.value.status == 3
+
+
+def test_mixed_projector_products_on_tensor_cores(cuda):
+    """Split-TF32 tcgen05 projector GEMMs (opt-in MIXED_TC form) against the FP64 cuBLAS path, Si64 (256 KB
+    projectors, K = 53,058 reals split over CTAs): the non-local term agrees to 1.5e-6 of its size
+    (FP32 accumulation in tensor memory; eigenvalue accuracy is checked in test_gpu_ditsp)."""
+    import torch
+    w = configs.si64_cubic()
+    d = configs.kpoint_inputs(w, 0)
+    nb = 160
+    psi = torch.from_numpy(np.ascontiguousarray(configs.random_psi(d["mtxd"], nb, 3).T)).to(cuda).t()
+    out = {}
+    for prec in (H.FP64, H.MIXED_TC):
+        ctx = H.Context(0, precision=prec).setup(d)
+        full = torch.zeros((nb, d["mtxd"]), dtype=torch.complex128, device=cuda).t()
+        loc = torch.zeros_like(full)
+        ctx.hk_psi(psi, full)
+        ctx.hk_psi(psi, loc, local_only=True)
+        torch.cuda.synchronize()
+        ctx.synchronize()
+        kin = torch.from_numpy(d["ekpg"]).to(cuda)[:, None] * psi
+        out[prec] = (full - loc - kin).cpu().numpy()       # the projector term
+    ref = out[H.FP64]
+    assert relerr(out[H.MIXED_TC], ref) < 1.5e-6
