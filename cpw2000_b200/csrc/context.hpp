@@ -93,8 +93,8 @@ struct cpw_b200_ctx {
   cpwb::DevBuf anl, anld, proj;
   std::vector<double> xnl_h;    // host copy of xnlkb
   // mixed precision: split-TF32 operands of the tensor-core projector GEMMs
-  cpwb::DevBuf tc_a1, tc_a2, tc_part, tc_b2, tc_err;
-  long long tc_k1p = 0, tc_k2p = 0;
+  cpwb::DevBuf tc_a1, tc_a2, tc_b1, tc_part, tc_b2, tc_err;
+  long long tc_k1p = 0, tc_k2p = 0;     // K blocks (32 reals) of the projection and expansion operands
   bool tc_ready = false;
 
   cpwb::StageTimer timer;

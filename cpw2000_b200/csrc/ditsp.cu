@@ -279,8 +279,10 @@ struct Solver {
   int lwork = 0;
   long long ihk = 0;
   int status = kOk;
-  // wall-clock accounting per phase (printed when ipr > 1): 0 H|psi>, 1 Gram-Schmidt, 2 subspace eigensolve
-  double tphase[4] = {0, 0, 0, 0};
+  // wall-clock accounting per phase (printed when ipr > 1): 0 H|psi>, 1 Gram-Schmidt, 2 subspace eigensolve;
+  // inside 1: 3 modified Gram-Schmidt leaves, 4 block passes against the converged vectors
+  double tphase[5] = {0, 0, 0, 0, 0};
+  long long n_gs = 0, n_gs_vec = 0, n_leaf = 0;
   bool timing = false;
   struct Tick {
     Solver* s;
@@ -395,6 +397,8 @@ struct Solver {
   int mgs_grid = 0;
   int grsch_mod(bool also, Z* x, Z* hx, int nvec, int* irow, const double* xscl) {
     if (nvec <= 0) return kOk;
+    Tick tk(this, 3);
+    ++n_leaf;
     if (!mgs_grid) {
       int dev = 0, nsm = 0, per = 0;
       cudaGetDevice(&dev);
@@ -484,11 +488,14 @@ struct Solver {
     irow.assign(std::max(nvec, 0), 1);
     if (nvec <= nconv) return kOk;
     const int k = nvec - nconv;
+    ++n_gs;
+    n_gs_vec += k;
     std::vector<zc> d;
     if (int s = coldots(x + (size_t)nconv * m, m, x + (size_t)nconv * m, m, k, d)) return s;
     std::vector<double> xscl(k);
     for (int i = 0; i < k; ++i) xscl[i] = d[i].real();
     if (nconv > 0) {
+      Tick tk4(this, 4);
       if (int s = smallA.ensure(sizeof(Z) * (size_t)nconv * k)) return s;
       Z* t = (Z*)smallA.p;
       for (int pass = 0; pass < 2; ++pass) {
@@ -1056,6 +1063,9 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
     printf("  ditsp_c16: %lld H|psi> band products, total %.4f s: H|psi> %.4f s, Gram-Schmidt %.4f s, "
            "subspace eigensolve %.4f s, other %.4f s\n",
            S.ihk, tot, S.tphase[0], S.tphase[1], S.tphase[2], tot - S.tphase[0] - S.tphase[1] - S.tphase[2]);
+    printf("  ditsp_c16: Gram-Schmidt %lld calls, %lld vectors: passes against converged %.4f s, "
+           "%lld modified Gram-Schmidt leaves %.4f s\n",
+           S.n_gs, S.n_gs_vec, S.tphase[4], S.n_leaf, S.tphase[3]);
     fflush(stdout);
   }
   if (S.sol) cusolverDnDestroy(S.sol);

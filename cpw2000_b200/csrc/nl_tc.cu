@@ -1,30 +1,46 @@
 // Mixed-precision KB projector products on the 5th-generation tensor cores.
 //
 // The complex products of Src/cpw_lib/hk_psi_nl_c16.f90:82-97 written as real
-// GEMMs in split TF32 (x = hi + lo, both TF32; a.b ~ hi.hi + hi.lo + lo.hi with
-// FP32 accumulation in tensor memory, ~2^-21 relative per product):
+// GEMMs in split TF32 (x = hi + lo, both TF32; a.b ~ hi.hi + hi.lo + lo.hi):
 //
-//   1. P = X^H psi:  [Re P; Im P] (2 nanl x nb) = A1 (2 nanl x 2 mtxd) . psi_interleaved
+//   1. P = X^H psi:  [Re P; Im P] (2 nanl x nb) = A1 (2 nanl x 2 mtxd) . B1^T
 //      A1 row a      = (xr_1, xi_1, xr_2, xi_2, ...) of projector a
 //      A1 row nanl+a = (-xi_1, xr_1, ...)
-//      psi is read in FP64 and split while it is staged into shared memory.
-//      Split over K across CTAs, FP32 partials summed in FP64 by k_reduce_p.
-//   2. hpsi += (X D) P: [Re | Im] (mtxd x 2 nb) = A2 (mtxd x 2 nanl) . B2^T with
-//      A2 row i = (xd_r(i, :), xd_i(i, :)), B2 row n = (Pr(:,n), -Pi(:,n)),
-//      B2 row nb+n = (Pi(:,n), Pr(:,n)); the epilogue adds into the FP64 hpsi.
+//      B1 row n      = (psi_r(1,n), psi_i(1,n), ...), split by k_split_psi.
+//      Split over K across work items; FP64 partials summed by k_reduce_p.
+//   2. hpsi += (X D) P: (mtxd x 2 nb) = A2 (mtxd x 2 nanl) . B2^T with
+//      A2 row i = (xd_r(i, :), xd_i(i, :)), B2 row 2n = (Pr(:,n), -Pi(:,n)),
+//      B2 row 2n+1 = (Pi(:,n), Pr(:,n)): output columns 2n, 2n+1 are the real and
+//      imaginary parts of hpsi(:, n), added in FP64.
 //
-// Kernel: one CTA of 4 warps per 128 x 128 output tile (and K range); 32-wide
-// K blocks staged (global -> registers -> shared, 128-byte swizzle) into two
-// buffers; thread 0 issues tcgen05.mma kind::tf32 (M 128, N 128, K 8) and
-// commits each block to an mbarrier; the other buffer is refilled meanwhile.
-// The accumulator lives in 128 TMEM columns and is read back with
-// tcgen05.ld 32x32b. Every mbarrier wait is bounded: on timeout the kernel sets
-// an error flag, skips its epilogue, frees its TMEM and returns.
+// Operand layout in HBM ("tiled"): every operand is stored as 128-row x 32-float
+// tiles, tile (row block rb, K block kb) at ((rb * nkb + kb) * 4096) floats, each
+// tile already in the 128-byte-swizzled K-major order the tensor cores read
+// (row r at r * 128 bytes, 16-byte chunk c at (c ^ (r & 7)) * 16). One pipeline
+// stage is then four contiguous bulk copies (cp.async.bulk, no tensor map) of
+// rows x 128 bytes, whole DRAM pages instead of 128-byte pieces of 128 rows.
+//
+// Kernel (persistent: grid <= SM count, work items = output tile x K range, 10 warps):
+//   warp 0      producer: bulk copies of A hi/lo and B hi/lo into a 3-stage ring
+//               (full/empty mbarriers);
+//   warp 1      allocates 512 TMEM columns; one lane issues tcgen05.mma kind::tf32
+//               (M 128, K 8): A hi . [B hi; B lo] as one N = 2 n MMA into adjacent
+//               main (hi.hi) and correction (hi.lo) columns, then A lo . B hi into
+//               the correction columns; two such accumulator pairs alternate;
+//   warps 2-9   drain: every `chain` K blocks they read a finished pair with
+//               tcgen05.ld, add main + correction in FP32 and accumulate in FP64
+//               registers (one row and 64 columns per thread), release the pair,
+//               and store the tile after its last chunk.
+// The FP32 accumulation of the tensor cores carries a systematic rounding bias
+// (measured: it grows with the number of accumulation steps into one accumulator);
+// draining every `chain` blocks keeps the steps per FP32 chain at 4 x chain while
+// the K range per work item stays long. Every mbarrier wait is bounded in time: on
+// timeout the kernel sets an error flag, skips its stores, waits (bounded) for its
+// copies and MMAs in flight, frees its TMEM and returns.
 #include <stdint.h>
 #include <stdlib.h>
 
 #include <algorithm>
-#include <string>
 
 #include "context.hpp"
 
@@ -32,33 +48,69 @@ namespace cpwb {
 namespace tc {
 
 constexpr int BM = 128, BN = 128, BK = 32;
-constexpr int kThreads = 128;
-constexpr int kTileBytes = BM * BK * 4;            // 16 KB per operand tile
-constexpr int kStageBytes = 4 * kTileBytes;        // A hi/lo + B hi/lo
-constexpr int kSmemBytes = 2 * kStageBytes + 1024 + 64;
-constexpr long long kWaitLimit = 1LL << 22;
-constexpr int kMainAcc = 3;                        // hi.hi accumulators; + 1 for the corrections
-constexpr int kTmemCols = (kMainAcc + 1) * BN;     // 512 columns
+constexpr int kStages = 3;
+constexpr int kTileFloats = BM * BK;               // 4096 floats = 16 KB
+constexpr int kTileBytes = kTileFloats * 4;
+constexpr int kStageBytes = 4 * kTileBytes;        // A hi, A lo, B hi, B lo
+constexpr int kDrainWarps = 8;
+constexpr int kThreads = 32 * (2 + kDrainWarps);
+constexpr int kBarBytes = 256;
+constexpr int kPrefetch = 8;                       // K blocks fetched into L2 ahead of the shared-memory copies
+constexpr int kEpiBytes = 2048;                    // per drain warp: 4 complex columns x 32 rows of FP64 staging
+constexpr int kSmemBytes = kStages * kStageBytes + 1024 + kBarBytes + kDrainWarps * kEpiBytes;
+constexpr unsigned long long kWaitNs = 2000000000ull;   // 2 s per mbarrier wait at most
+constexpr int kTmemCols = 512;                     // 2 x (main 128 + correction 128)
+
+// float offset of element (r, k) of a tiled operand with nkb K blocks
+__host__ __device__ __forceinline__ size_t tiled_off(long long r, long long k, long long nkb) {
+  return (size_t)(((r >> 7) * nkb + (k >> 5)) * kTileFloats) + (size_t)((r & 127) * 32) +
+         (size_t)(((((k >> 2) & 7) ^ (r & 7)) << 2) | (k & 3));
+}
 
 struct GemmArgs {
-  int M, N, K;                 // output rows / cols, reduction length
-  int kb_per_split;            // 32-wide K blocks per CTA (blockIdx.z)
-  const float* a_hi;           // M x lda, row-major, zero beyond K
+  const float* a_hi;           // tiled, rows M (padded to 128), nkb K blocks
   const float* a_lo;
-  long long lda;
-  const float* b_hi;           // N x ldb row-major (B source 0)
+  const float* b_hi;           // tiled, rows N
   const float* b_lo;
-  long long ldb;
-  const double* b64;           // B source 1: row n = doubles b64[n*ldb64 ...], K reals per row
-  long long ldb64;
-  float* part;                 // mode 0: part[z][n][mpad]
-  long long mpad;
-  double* hpsi;                // mode 1: complex128 (interleaved), ld ldh complex elements
-  long long ldh;
-  int nbh;                     // mode 1: columns < nbh are real parts, >= nbh imaginary parts
+  int M, N;                    // output rows / columns
+  int nkb;                     // 32-wide K blocks in total
+  int kb_per_split;            // K blocks per work item
+  int nsplit;
+  int chain;                   // K blocks per FP32 accumulation chain
+  int tiles_m, tiles_n;
+  int n_fast;                  // tile order: 1 = consecutive items share an m tile
   int terms;                   // 3: hi.hi + hi.lo + lo.hi; 4: also lo.lo
+  double* out;                 // mode 0: out[split][n][M]; mode 1: complex128 hpsi, ld ldh
+  long long ldh;
   int* err;
 };
+
+struct Item {
+  int m0, n0, split, kb0, nblk, rows_a, rows_b, n_mma;
+};
+
+__device__ __forceinline__ Item item_of(const GemmArgs& g, int it) {
+  Item w;
+  const int tiles = g.tiles_m * g.tiles_n;
+  w.split = it / tiles;
+  const int tile = it - w.split * tiles;
+  int mt, nt;
+  if (g.n_fast) {
+    nt = tile % g.tiles_n;
+    mt = tile / g.tiles_n;
+  } else {
+    mt = tile % g.tiles_m;
+    nt = tile / g.tiles_m;
+  }
+  w.m0 = mt * BM;
+  w.n0 = nt * BN;
+  w.kb0 = w.split * g.kb_per_split;
+  w.nblk = max(0, min(g.nkb, w.kb0 + g.kb_per_split) - w.kb0);
+  w.rows_a = min(BM, g.M - w.m0);
+  w.rows_b = min(BN, g.N - w.n0);
+  w.n_mma = min(BN, ((w.rows_b + 15) / 16) * 16);
+  return w;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -68,9 +120,7 @@ __device__ __forceinline__ float tf32(float x) {
   return __uint_as_float(r);
 }
 
-// K-major, 128-byte swizzled tile of rows x 32 fp32: row r, 16-byte chunk c
-__device__ __forceinline__ int sw_off(int r, int c) { return r * 128 + ((c ^ (r & 7)) << 4); }
-
+// K-major operand tile, 128-byte swizzle: 8-row groups 1024 bytes apart
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
   uint64_t d = 0;
   d |= (uint64_t)((addr >> 4) & 0x3FFF);               // start address
@@ -81,11 +131,11 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
   return d;
 }
 
-__device__ __forceinline__ uint32_t instr_desc() {
+__device__ __forceinline__ uint32_t instr_desc(int n) {
   return (1u << 4)                  // D format F32
          | (2u << 7)                // A TF32
          | (2u << 10)               // B TF32
-         | ((uint32_t)(BN >> 3) << 17)
+         | ((uint32_t)(n >> 3) << 17)
          | ((uint32_t)(BM >> 4) << 24);
 }
 
@@ -102,82 +152,104 @@ __device__ __forceinline__ void mma_commit(uint32_t mbar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mbar) : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-  for (long long it = 0; it < kWaitLimit; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(done)
-        : "r"(mbar), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
+__device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(done)
+      : "r"(mbar), "r"(parity)
+      : "memory");
+  return done != 0;
 }
 
-// stage rows [r0, r0+128) x K block kb of a row-major FP32 hi/lo pair
-__device__ __forceinline__ void load_split(unsigned char* hi_t, unsigned char* lo_t, const float* hi, const float* lo,
-                                          long long ld, int rows, int r0, int k0) {
-  for (int idx = threadIdx.x; idx < BM * 8; idx += kThreads) {
-    const int r = idx >> 3, c = idx & 7;
-    float4 vh = make_float4(0.f, 0.f, 0.f, 0.f), vl = vh;
-    if (r0 + r < rows) {
-      const size_t o = (size_t)(r0 + r) * ld + k0 + 4 * c;
-      vh = *reinterpret_cast<const float4*>(hi + o);
-      vl = *reinterpret_cast<const float4*>(lo + o);
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// wait bounded in time; gives up early once another role has recorded a failure
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, const volatile int* failed) {
+  const unsigned long long t0 = globaltimer_ns();
+  for (unsigned it = 0;; ++it) {
+    if (mbar_try(mbar, parity)) return true;
+    if ((it & 63) == 63) {
+      if (failed && *failed) return false;
+      if (globaltimer_ns() - t0 > kWaitNs) return false;
     }
-    *reinterpret_cast<float4*>(hi_t + sw_off(r, c)) = vh;
-    *reinterpret_cast<float4*>(lo_t + sw_off(r, c)) = vl;
   }
 }
 
-// stage rows of an FP64 source, splitting into TF32 hi/lo on the way
-__device__ __forceinline__ void load_fp64(unsigned char* hi_t, unsigned char* lo_t, const double* src, long long ld,
-                                         int rows, int K, int r0, int k0) {
-  for (int idx = threadIdx.x; idx < BN * 8; idx += kThreads) {
-    const int r = idx >> 3, c = idx & 7;
-    float h[4] = {0.f, 0.f, 0.f, 0.f}, l[4] = {0.f, 0.f, 0.f, 0.f};
-    if (r0 + r < rows) {
-      const double* row = src + (size_t)(r0 + r) * ld;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int k = k0 + 4 * c + j;
-        if (k < K) {
-          const double x = row[k];
-          const float xh = tf32((float)x);
-          h[j] = xh;
-          l[j] = tf32((float)(x - (double)xh));
-        }
-      }
-    }
-    *reinterpret_cast<float4*>(hi_t + sw_off(r, c)) = make_float4(h[0], h[1], h[2], h[3]);
-    *reinterpret_cast<float4*>(lo_t + sw_off(r, c)) = make_float4(l[0], l[1], l[2], l[3]);
-  }
+__device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mbar), "r"(count));
 }
 
-template <int BSRC, int MODE>
-__global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(GemmArgs g) {
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+// contiguous global -> shared bulk copy (16-byte aligned, size a multiple of 16), no multicast
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(mbar)
+               : "memory");
+}
+
+__device__ __forceinline__ void prefetch_l2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(src), "r"(bytes) : "memory");
+}
+
+// global[dst .. dst+bytes) += shared[src ..] in FP64, performed by the memory system
+__device__ __forceinline__ void bulk_add_f64(void* dst, uint32_t src, uint32_t bytes) {
+  asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f64 [%0], [%1], %2;\n" ::"l"(dst), "r"(src),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
   extern __shared__ unsigned char smem_raw[];
-  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  unsigned char* tiles = base;                                     // 2 stages x (A hi, A lo, B hi, B lo)
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(base + 2 * kStageBytes);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(base + 2 * kStageBytes + 16);
-  __shared__ int failed;
+  unsigned char* tiles = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tiles + kStages * kStageBytes);
+  uint64_t* full = bars;                     // [kStages] copies landed
+  uint64_t* empty = bars + kStages;          // [kStages] MMAs that read the stage are done
+  uint64_t* accf = bars + 2 * kStages;       // [2] accumulator pair ready for the drain
+  uint64_t* acce = accf + 2;                 // [2] accumulator pair drained
+  uint64_t* done = acce + 2;                 // all MMAs of this CTA complete
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+  unsigned char* epi = tiles + kStages * kStageBytes + kBarBytes;   // drain-warp staging (mode 1)
+  __shared__ volatile int failed;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-  const int nkb_total = (g.K + BK - 1) / BK;
-  const int kb0 = blockIdx.z * g.kb_per_split;
-  const int kb1 = min(nkb_total, kb0 + g.kb_per_split);
+  const int nitems = g.tiles_m * g.tiles_n * g.nsplit;
+  const int chain = max(1, g.chain);
+  const size_t nkb = (size_t)g.nkb;
 
   if (threadIdx.x == 0) {
     failed = 0;
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mbar[0])));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mbar[1])));
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(smem_u32(&full[s]), 1);
+      mbar_init(smem_u32(&empty[s]), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&accf[b]), 1);
+      mbar_init(smem_u32(&acce[b]), kDrainWarps);
+    }
+    mbar_init(smem_u32(done), 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  if (warp == 0) {
+  if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tslot)),
                  "r"(kTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
@@ -186,180 +258,313 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(GemmArgs g) {
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n");
   const uint32_t tmem = *tslot;
-  const uint32_t idesc = instr_desc();
 
-  const int nblk = kb1 - kb0;
-  for (int i = 0; i < nblk; ++i) {
-    const int s = i & 1;
-    unsigned char* st = tiles + s * kStageBytes;
-    if (i >= 2) {
-      // the MMAs that read this stage two blocks ago must be finished
-      if (!mbar_wait(smem_u32(&mbar[s]), (uint32_t)(((i - 2) >> 1) & 1))) {
-        if (threadIdx.x == 0) atomicExch(g.err, 1);
-        failed = 1;
+  if (warp == 0) {
+    if (lane == 0) {
+      long long gk = 0;                      // K blocks issued by this CTA (ring position)
+      for (int it = blockIdx.x; it < nitems && !failed; it += gridDim.x) {
+        const Item w = item_of(g, it);
+        const float* ah = g.a_hi + (size_t)(w.m0 >> 7) * nkb * kTileFloats;
+        const float* al = g.a_lo + (size_t)(w.m0 >> 7) * nkb * kTileFloats;
+        const float* bh = g.b_hi + (size_t)(w.n0 >> 7) * nkb * kTileFloats;
+        const float* bl = g.b_lo + (size_t)(w.n0 >> 7) * nkb * kTileFloats;
+        const uint32_t bytes_a = (uint32_t)w.rows_a * 128u, bytes_b = (uint32_t)w.rows_b * 128u;
+        auto prefetch = [&](int i) {
+          const size_t o = (size_t)(w.kb0 + i) * kTileFloats;
+          prefetch_l2(ah + o, bytes_a);
+          prefetch_l2(al + o, bytes_a);
+          prefetch_l2(bh + o, bytes_b);
+          prefetch_l2(bl + o, bytes_b);
+        };
+        for (int i = 0; i < min(kPrefetch, w.nblk); ++i) prefetch(i);
+        for (int i = 0; i < w.nblk; ++i, ++gk) {
+          if (i + kPrefetch < w.nblk) prefetch(i + kPrefetch);
+          const int s = (int)(gk % kStages);
+          const long long r = gk / kStages;
+          if (r > 0 && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((r - 1) & 1), &failed)) {
+            failed = 1;
+            atomicExch(g.err, 1);
+            break;
+          }
+          unsigned char* st = tiles + s * kStageBytes;
+          const uint32_t fb = smem_u32(&full[s]);
+          mbar_expect_tx(fb, 2u * (bytes_a + bytes_b));
+          const size_t o = (size_t)(w.kb0 + i) * kTileFloats;
+          bulk_load(smem_u32(st), ah + o, bytes_a, fb);
+          bulk_load(smem_u32(st + kTileBytes), al + o, bytes_a, fb);
+          // B lo rows follow the n_mma B hi rows: one N = 2 n_mma MMA reads [B hi; B lo]
+          bulk_load(smem_u32(st + 2 * kTileBytes), bh + o, bytes_b, fb);
+          bulk_load(smem_u32(st + 2 * kTileBytes + w.n_mma * 128), bl + o, bytes_b, fb);
+        }
       }
-      __syncthreads();
-      if (failed) break;
+      // copies still in flight land before the CTA may exit
+      for (long long i = (gk > kStages ? gk - kStages : 0); i < gk; ++i)
+        if (!mbar_wait(smem_u32(&full[i % kStages]), (uint32_t)((i / kStages) & 1), nullptr)) atomicExch(g.err, 1);
     }
-    const int k0 = (kb0 + i) * BK;
-    load_split(st, st + kTileBytes, g.a_hi, g.a_lo, g.lda, g.M, m0, k0);
-    if (BSRC == 0)
-      load_split(st + 2 * kTileBytes, st + 3 * kTileBytes, g.b_hi, g.b_lo, g.ldb, g.N, n0, k0);
-    else
-      load_fp64(st + 2 * kTileBytes, st + 3 * kTileBytes, g.b64, g.ldb64, g.N, g.K, n0, k0);
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;\n");
-      const uint32_t ah = smem_u32(st), al = smem_u32(st + kTileBytes);
-      const uint32_t bh = smem_u32(st + 2 * kTileBytes), bl = smem_u32(st + 3 * kTileBytes);
-      // hi.hi into main accumulator i % 3 (round-robin keeps each FP32 chain short),
-      // the small correction products into the fourth accumulator
-      const uint32_t tmain = tmem + (uint32_t)((i % kMainAcc) * BN);
-      const uint32_t tcorr = tmem + (uint32_t)(kMainAcc * BN);
+  } else if (warp == 1) {
+    if (lane == 0) {
+      long long gk = 0;                      // K blocks consumed
+      long long gq = 0;                      // accumulation chunks issued
+      for (int it = blockIdx.x; it < nitems && !failed; it += gridDim.x) {
+        const Item w = item_of(g, it);
+        const uint32_t idesc = instr_desc(w.n_mma), idesc2 = instr_desc(2 * w.n_mma);
+        const int nchunk = (w.nblk + chain - 1) / chain;
+        for (int q = 0; q < nchunk && !failed; ++q, ++gq) {
+          const int b = (int)(gq & 1);
+          if (gq >= 2 && !mbar_wait(smem_u32(&acce[b]), (uint32_t)(((gq >> 1) - 1) & 1), &failed)) {
+            failed = 1;
+            atomicExch(g.err, 1);
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;\n");
+          // buffer b: columns [b*256, +n_mma) hi.hi, [b*256 + n_mma, +n_mma) hi.lo + lo.hi
+          const uint32_t tmain = tmem + (uint32_t)(b * 2 * BN), tcorr = tmain + (uint32_t)w.n_mma;
+          const int i0 = q * chain, i1 = min(w.nblk, i0 + chain);
+          bool ok = true;
+          for (int i = i0; i < i1; ++i, ++gk) {
+            const int s = (int)(gk % kStages);
+            if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((gk / kStages) & 1), &failed)) {
+              ok = false;
+              break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;\n");
+            unsigned char* st = tiles + s * kStageBytes;
+            const uint32_t ah = smem_u32(st), al = smem_u32(st + kTileBytes);
+            const uint32_t bh = smem_u32(st + 2 * kTileBytes), bl = bh + (uint32_t)w.n_mma * 128u;
 #pragma unroll
-      for (int ks = 0; ks < BK / 8; ++ks) {
-        const uint32_t off = ks * 32;       // 8 tf32 = 32 bytes along K inside the swizzled row
-        mma_tf32(tmain, smem_desc(ah + off), smem_desc(bh + off), idesc, (i < kMainAcc && ks == 0) ? 0u : 1u);
-        mma_tf32(tcorr, smem_desc(ah + off), smem_desc(bl + off), idesc, (i == 0 && ks == 0) ? 0u : 1u);
-        mma_tf32(tcorr, smem_desc(al + off), smem_desc(bh + off), idesc, 1u);
-        if (g.terms > 3) mma_tf32(tcorr, smem_desc(al + off), smem_desc(bl + off), idesc, 1u);
+            for (int ks = 0; ks < BK / 8; ++ks) {
+              const uint32_t off = ks * 32;     // 8 tf32 = 32 bytes along K inside the swizzled row
+              const uint32_t acc = (i == i0 && ks == 0) ? 0u : 1u;
+              mma_tf32(tmain, smem_desc(ah + off), smem_desc(bh + off), idesc2, acc);   // A hi . [B hi; B lo]
+              mma_tf32(tcorr, smem_desc(al + off), smem_desc(bh + off), idesc, 1u);     // A lo . B hi
+              if (g.terms > 3) mma_tf32(tcorr, smem_desc(al + off), smem_desc(bl + off), idesc, 1u);
+            }
+            mma_commit(smem_u32(&empty[s]));
+          }
+          if (!ok) {
+            failed = 1;
+            atomicExch(g.err, 1);
+            break;
+          }
+          mma_commit(smem_u32(&accf[b]));
+        }
       }
-      mma_commit(smem_u32(&mbar[s]));
+      // every MMA of this thread completes before TMEM is freed
+      mma_commit(smem_u32(done));
+      if (!mbar_wait(smem_u32(done), 0u, nullptr)) atomicExch(g.err, 1);
     }
-  }
-  // wait for the last block's MMAs (they complete after all earlier ones)
-  if (nblk > 0 && !failed) {
-    const int last = nblk - 1;
-    if (!mbar_wait(smem_u32(&mbar[last & 1]), (uint32_t)((last >> 1) & 1))) {
-      if (threadIdx.x == 0) atomicExch(g.err, 1);
-      failed = 1;
-    }
-  }
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;\n");
-  if (!failed && nblk > 0) {
-    const int m = m0 + warp * 32 + lane;
-    const int nacc = min(nblk, kMainAcc);
-    for (int c0 = 0; c0 < BN; c0 += 16) {
-      double acc[16];
+  } else {
+    const int quarter = warp & 3, half = (warp - 2) >> 2;
+    const uint32_t lane_base = tmem + ((uint32_t)(32 * quarter) << 16);
+    long long gq = 0;
+    for (int it = blockIdx.x; it < nitems && !failed; it += gridDim.x) {
+      const Item w = item_of(g, it);
+      const int nchunk = (w.nblk + chain - 1) / chain;
+      double acc[64];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) acc[j] = 0.0;
-      for (int a = 0; a <= kMainAcc; ++a) {
-        if (a < kMainAcc && a >= nacc) continue;      // main accumulators that never received a block
-        uint32_t r[16];
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(a * BN + c0);
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-            : "r"(taddr));
-        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      for (int j = 0; j < 64; ++j) acc[j] = 0.0;
+      bool ok = true;
+      for (int q = 0; q < nchunk; ++q, ++gq) {
+        const int b = (int)(gq & 1);
+        if (!mbar_wait(smem_u32(&accf[b]), (uint32_t)((gq >> 1) & 1), &failed)) {
+          ok = false;
+          failed = 1;
+          atomicExch(g.err, 1);
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;\n");
 #pragma unroll
-        for (int j = 0; j < 16; ++j) acc[j] += (double)__uint_as_float(r[j]);
+        for (int j = 0; j < 8; ++j) {
+          const int col = 64 * half + 8 * j;
+          if (col < w.n_mma) {          // n_mma is a multiple of 16: whole 8-column pieces
+            uint32_t rm[8], rc[8];
+            tmem_ld8(lane_base + (uint32_t)(b * 2 * BN + col), rm);
+            tmem_ld8(lane_base + (uint32_t)(b * 2 * BN + w.n_mma + col), rc);
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+            for (int t = 0; t < 8; ++t) acc[8 * j + t] += (double)(__uint_as_float(rm[t]) + __uint_as_float(rc[t]));
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;\n");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&acce[b]));
       }
-      if (m < g.M) {
+      if (!ok || failed) break;
+      const int m = w.m0 + 32 * quarter + lane;
+      if (nchunk > 0 && w.m0 + 32 * quarter < g.M) {      // warp-uniform: the warp has valid rows
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int n = n0 + c0 + j;
-          if (n >= g.N) continue;
-          const double v = acc[j];
-          if (MODE == 0) {
-            g.part[((size_t)blockIdx.z * g.N + n) * g.mpad + m] = (float)v;
-          } else {
-            const int col = n < g.nbh ? n : n - g.nbh;
-            double* dst = g.hpsi + 2 * ((size_t)col * g.ldh + m) + (n < g.nbh ? 0 : 1);
-            *dst += v;
+        for (int j = 0; j < 4; ++j) {
+          const int col = 64 * half + 16 * j;
+          if (col < w.n_mma) {
+            if (MODE == 0) {
+#pragma unroll
+              for (int t = 0; t < 16; ++t) {
+                const int n = w.n0 + col + t;
+                if (n < g.N && m < g.M) g.out[((size_t)w.split * g.N + n) * g.M + m] = acc[16 * j + t];
+              }
+            } else {
+              // four complex columns at a time through this warp's staging slot: [column][32 rows] of
+              // (re, im), then one bulk FP64 add of 32 rows (512 contiguous bytes of hpsi) per column
+              double2* slot = reinterpret_cast<double2*>(epi + (warp - 2) * kEpiBytes);
+              const int rows = min(32, g.M - (w.m0 + 32 * quarter));
+#pragma unroll
+              for (int hh = 0; hh < 2; ++hh) {
+                const int c0 = w.n0 + col + 8 * hh;           // first real output column of the four
+                // the previous bulk adds must have finished reading the slot
+                asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+                __syncwarp();
+#pragma unroll
+                for (int t = 0; t < 4; ++t)
+                  slot[t * 32 + lane] = make_double2(acc[16 * j + 8 * hh + 2 * t], acc[16 * j + 8 * hh + 2 * t + 1]);
+                asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                __syncwarp();
+                if (lane == 0) {
+                  for (int t = 0; t < 4; ++t)
+                    if (c0 + 2 * t + 1 < g.N)
+                      bulk_add_f64(reinterpret_cast<double2*>(g.out) + (size_t)((c0 >> 1) + t) * g.ldh + (m - lane),
+                                   smem_u32(slot + t * 32), (uint32_t)rows * 16u);
+                  asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+                }
+              }
+            }
           }
         }
       }
     }
   }
+  if (MODE == 1 && warp >= 2 && lane == 0) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;\n");
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTmemCols));
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTmemCols));
+  }
 }
 
-// A1 (2 nanl x k1p) and A2 (mtxd x k2p) TF32 hi/lo from X (anl) and X D (anld), complex128 ld mtxd
-__global__ void k_prep_a1(int mtxd, int nanl, long long k1p, const C2<double>* __restrict__ x, float* __restrict__ hi,
-                          float* __restrict__ lo) {
-  const long long n = 2LL * nanl * k1p;
+__device__ __forceinline__ void put_split(float* hi, float* lo, size_t o, double v0, double v1) {
+  const float h0 = tf32((float)v0), h1 = tf32((float)v1);
+  *reinterpret_cast<float2*>(hi + o) = make_float2(h0, h1);
+  *reinterpret_cast<float2*>(lo + o) = make_float2(tf32((float)(v0 - (double)h0)), tf32((float)(v1 - (double)h1)));
+}
+
+// B1 (nb rows, K = 2 mtxd reals, tiled): row n = interleaved psi(:, n), zero beyond 2 mtxd
+__global__ void k_split_psi(int nb, int mtxd, long long nkb, const C2<double>* __restrict__ psi, long long ldpsi,
+                            float* __restrict__ hi, float* __restrict__ lo) {
+  const long long pairs = nkb * 16;                    // complex entries per padded row
+  const long long n = (long long)nb * pairs;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    const long long row = t / k1p, k = t - row * k1p;
+    const long long r = t / pairs, i = t - r * pairs;
+    C2<double> z = mk(0.0, 0.0);
+    if (i < mtxd) z = psi[(size_t)r * ldpsi + i];
+    put_split(hi, lo, tiled_off(r, 2 * i, nkb), z.x, z.y);
+  }
+}
+
+// A1 (2 nanl rows, K = 2 mtxd, tiled) from X (anl, complex128 ld mtxd)
+__global__ void k_prep_a1(int mtxd, int nanl, long long nkb, const C2<double>* __restrict__ x, float* __restrict__ hi,
+                          float* __restrict__ lo) {
+  const long long pairs = nkb * 16;
+  const long long n = 2LL * nanl * pairs;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const long long row = t / pairs, i = t - row * pairs;
     const int a = (int)(row % nanl);
-    const bool rot = row >= nanl;
-    const long long i = k >> 1;
-    double v = 0.0;
-    if (i < mtxd) {
-      const C2<double> z = x[(size_t)a * mtxd + i];
-      v = (k & 1) ? (rot ? z.x : z.y) : (rot ? -z.y : z.x);
-    }
-    const float h = tf32((float)v);
-    hi[t] = h;
-    lo[t] = tf32((float)(v - (double)h));
+    C2<double> z = mk(0.0, 0.0);
+    if (i < mtxd) z = x[(size_t)a * mtxd + i];
+    if (row < nanl)
+      put_split(hi, lo, tiled_off(row, 2 * i, nkb), z.x, z.y);
+    else
+      put_split(hi, lo, tiled_off(row, 2 * i, nkb), -z.y, z.x);
   }
 }
 
-__global__ void k_prep_a2(int mtxd, int nanl, long long k2p, const C2<double>* __restrict__ xd, float* __restrict__ hi,
+// A2 (mtxd rows, K = 2 nanl, tiled) from X D (anld): row i = (xd_r(i, :), xd_i(i, :))
+__global__ void k_prep_a2(int mtxd, int nanl, long long nkb, const C2<double>* __restrict__ xd, float* __restrict__ hi,
                           float* __restrict__ lo) {
-  const long long n = (long long)mtxd * k2p;
+  const long long pairs = nkb * 16;                    // K pairs per padded row
+  const long long n = (long long)mtxd * pairs;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    const long long i = t / k2p, k = t - i * k2p;
-    double v = 0.0;
-    if (k < 2 * nanl) {
-      const int a = (int)(k % nanl);
-      const C2<double> z = xd[(size_t)a * mtxd + i];
-      v = k < nanl ? z.x : z.y;
+    const long long i = t / pairs, k = 2 * (t - i * pairs);
+    double v[2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const long long kk = k + e;
+      v[e] = 0.0;
+      if (kk < 2 * nanl) {
+        const int a = (int)(kk % nanl);
+        const C2<double> z = xd[(size_t)a * mtxd + i];
+        v[e] = kk < nanl ? z.x : z.y;
+      }
     }
-    const float h = tf32((float)v);
-    hi[t] = h;
-    lo[t] = tf32((float)(v - (double)h));
+    put_split(hi, lo, tiled_off(i, k, nkb), v[0], v[1]);
   }
 }
 
-// P from the split-K partials, and B2 (2 nb x k2p) TF32 hi/lo for the expansion GEMM
-__global__ void k_reduce_p(int nanl, int nb, int nsplit, long long mpad, long long k2p, const float* __restrict__ part,
-                           float* __restrict__ b2hi, float* __restrict__ b2lo) {
+// P from the FP64 split-K partials part[z][n][2 nanl]; B2 (2 nb rows, K = 2 nanl, tiled):
+// row 2n = (Pr, -Pi), row 2n+1 = (Pi, Pr). K entries beyond 2 nanl are cleared by the caller.
+__global__ void k_reduce_p(int nanl, int nb, int nsplit, long long nkb, const double* __restrict__ part,
+                           float* __restrict__ hi, float* __restrict__ lo) {
   const long long n = (long long)nanl * nb;
+  const long long m2 = 2LL * nanl;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    const int a = (int)(t % nanl), b = (int)(t / nanl);
+    const long long a = t % nanl, b = t / nanl;
     double pr = 0.0, pi = 0.0;
     for (int z = 0; z < nsplit; ++z) {
-      const float* pz = part + ((size_t)z * nb + b) * mpad;
+      const double* pz = part + ((size_t)z * nb + b) * m2;
       pr += pz[a];
       pi += pz[nanl + a];
     }
     auto put = [&](long long row, long long k, double v) {
       const float h = tf32((float)v);
-      b2hi[row * k2p + k] = h;
-      b2lo[row * k2p + k] = tf32((float)(v - (double)h));
+      const size_t o = tiled_off(row, k, nkb);
+      hi[o] = h;
+      lo[o] = tf32((float)(v - (double)h));
     };
-    put(b, a, pr);
-    put(b, nanl + a, -pi);
-    put(nb + b, a, pi);
-    put(nb + b, nanl + a, pr);
+    put(2 * b, a, pr);
+    put(2 * b, nanl + a, -pi);
+    put(2 * b + 1, a, pi);
+    put(2 * b + 1, nanl + a, pr);
   }
 }
 
+inline size_t tiled_floats(long long rows, long long nkb) { return (size_t)((rows + 127) / 128) * nkb * kTileFloats; }
+
 }  // namespace tc
+
+namespace {
+
+int env_int(const char* name, int dflt) {
+  const char* v = getenv(name);
+  return v ? atoi(v) : dflt;
+}
+
+int grid_for(long long work, int nsm) {
+  return (int)std::max(1LL, std::min((long long)(8 * nsm), (work + 255) / 256));
+}
+
+}  // namespace
 
 int tc_prepare_projectors(cpw_b200_ctx* c) {
   const int m = c->mtxd, na = c->nanl;
   if (na == 0 || m == 0) return kOk;
-  const long long k1p = ((2LL * m + tc::BK - 1) / tc::BK) * tc::BK;
-  const long long k2p = ((2LL * na + tc::BK - 1) / tc::BK) * tc::BK;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const long long nkb1 = (2LL * m + tc::BK - 1) / tc::BK;
+  const long long nkb2 = (2LL * na + tc::BK - 1) / tc::BK;
+  const size_t fa1 = tc::tiled_floats(2 * na, nkb1), fa2 = tc::tiled_floats(m, nkb2);
   int s;
-  if ((s = c->tc_a1.ensure(sizeof(float) * 2 * (size_t)(2 * na) * k1p)) ||
-      (s = c->tc_a2.ensure(sizeof(float) * 2 * (size_t)m * k2p)))
-    return s;
+  if ((s = c->tc_a1.ensure(sizeof(float) * 2 * fa1)) || (s = c->tc_a2.ensure(sizeof(float) * 2 * fa2))) return s;
   float* a1 = (float*)c->tc_a1.p;
   float* a2 = (float*)c->tc_a2.p;
-  tc::k_prep_a1<<<1184, 256, 0, c->stream>>>(m, na, k1p, (const C2<double>*)c->anl.p, a1, a1 + (size_t)2 * na * k1p);
-  tc::k_prep_a2<<<1184, 256, 0, c->stream>>>(m, na, k2p, (const C2<double>*)c->anld.p, a2, a2 + (size_t)m * k2p);
+  tc::k_prep_a1<<<grid_for(2LL * na * nkb1 * 16, nsm), 256, 0, c->stream>>>(m, na, nkb1, (const C2<double>*)c->anl.p,
+                                                                              a1, a1 + fa1);
+  tc::k_prep_a2<<<grid_for((long long)m * nkb2 * 16, nsm), 256, 0, c->stream>>>(m, na, nkb2,
+                                                                                 (const C2<double>*)c->anld.p, a2,
+                                                                                 a2 + fa2);
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "tensor-core projector preparation");
-  c->tc_k1p = k1p;
-  c->tc_k2p = k2p;
+  c->tc_k1p = nkb1;
+  c->tc_k2p = nkb2;
   c->tc_ready = true;
   return kOk;
 }
@@ -369,76 +574,89 @@ int tc_nl_apply(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void*
                 cudaEvent_t t0, cudaEvent_t t1, cudaEvent_t t2) {
   if (!c->tc_ready) return fail(kNotReady, "tensor-core projectors not prepared");
   const int m = c->mtxd, na = c->nanl;
-  const long long k1p = c->tc_k1p, k2p = c->tc_k2p;
+  const long long nkb1 = c->tc_k1p, nkb2 = c->tc_k2p;
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  // GEMM 1: (2 nanl) x nb, K = 2 mtxd, split over K
+  const int chain = std::max(1, env_int("CPW_B200_TC_CHAIN", 4));
+  const int terms = env_int("CPW_B200_TC_TERMS", 3) == 4 ? 4 : 3;
+
+  // GEMM 1: (2 nanl) x nb, K = 2 mtxd, split over K so that the work items fill the SMs about once
   const int mt1 = (2 * na + tc::BM - 1) / tc::BM, nt1 = (nb + tc::BN - 1) / tc::BN;
-  const int nkb = (int)(k1p / tc::BK);
-  // K blocks per CTA of the projection: at most 16 (three main accumulators of <= 6 blocks each keep the
-  // FP32 accumulation bias of the tensor cores near 5e-7 relative), fewer when the grid is too small
-  int nsplit = std::max(1, std::min(nkb, (2 * nsm) / std::max(1, mt1 * nt1)));
-  int kbps = std::min(16, (nkb + nsplit - 1) / nsplit);
-  // tuning: K blocks per CTA (shorter chains are more accurate, longer ones write fewer partials)
-  if (const char* ev = getenv("CPW_B200_TC_KBLOCKS")) kbps = std::max(1, std::min(nkb, atoi(ev)));
-  nsplit = (nkb + kbps - 1) / kbps;
-  const long long mpad = (long long)mt1 * tc::BM;
+  int nsplit = std::max(1, (int)std::min<long long>(nkb1, nsm / (mt1 * nt1)));
+  if (const int ks = env_int("CPW_B200_TC_SPLITS", 0)) nsplit = (int)std::max(1LL, std::min<long long>(nkb1, ks));
+  const int kbps = (int)((nkb1 + nsplit - 1) / nsplit);
+  nsplit = (int)((nkb1 + kbps - 1) / kbps);
+  const size_t fb1 = tc::tiled_floats(nb, nkb1), fb2 = tc::tiled_floats(2 * nb, nkb2);
   int s;
-  if ((s = c->tc_part.ensure(sizeof(float) * (size_t)nsplit * nb * mpad)) ||
-      (s = c->tc_b2.ensure(sizeof(float) * 2 * (size_t)(2 * nb) * k2p)) || (s = c->tc_err.ensure(sizeof(int))))
+  if ((s = c->tc_b1.ensure(sizeof(float) * 2 * fb1)) ||
+      (s = c->tc_part.ensure(sizeof(double) * (size_t)nsplit * nb * 2 * na)) ||
+      (s = c->tc_b2.ensure(sizeof(float) * 2 * fb2)) || (s = c->tc_err.ensure(sizeof(int))))
     return s;
-  cudaError_t e = cudaMemsetAsync(c->tc_err.p, 0, sizeof(int), st);
-  if (e != cudaSuccess) return cuda_fail(e, "tc nl");
-  // B2 rows beyond 2 nanl in K must be zero: clear once per call (small)
-  e = cudaMemsetAsync(c->tc_b2.p, 0, sizeof(float) * 2 * (size_t)(2 * nb) * k2p, st);
-  if (e != cudaSuccess) return cuda_fail(e, "tc nl");
-  if ((e = cudaFuncSetAttribute(tc::k_gemm_tf32x3<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                tc::kSmemBytes)) != cudaSuccess ||
-      (e = cudaFuncSetAttribute(tc::k_gemm_tf32x3<0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                tc::kSmemBytes)) != cudaSuccess)
-    return cuda_fail(e, "tensor-core GEMM attribute");
+  float* b1 = (float*)c->tc_b1.p;
+  float* b2 = (float*)c->tc_b2.p;
+  const float* a1 = (const float*)c->tc_a1.p;
+  const float* a2 = (const float*)c->tc_a2.p;
+  const size_t fa1 = tc::tiled_floats(2 * na, nkb1), fa2 = tc::tiled_floats(m, nkb2);
+
   tc::GemmArgs g1{};
+  g1.a_hi = a1;
+  g1.a_lo = a1 + fa1;
+  g1.b_hi = b1;
+  g1.b_lo = b1 + fb1;
   g1.M = 2 * na;
   g1.N = nb;
-  g1.K = 2 * m;
+  g1.nkb = (int)nkb1;
   g1.kb_per_split = kbps;
-  g1.a_hi = (const float*)c->tc_a1.p;
-  g1.a_lo = g1.a_hi + (size_t)2 * na * k1p;
-  g1.lda = k1p;
-  g1.b64 = (const double*)psi;
-  g1.ldb64 = 2 * ldpsi;
-  g1.part = (float*)c->tc_part.p;
-  g1.mpad = mpad;
-  g1.err = (int*)c->tc_err.p;
-  int terms = 3;
-  if (const char* ev = getenv("CPW_B200_TC_TERMS")) terms = atoi(ev) == 4 ? 4 : 3;
+  g1.nsplit = nsplit;
+  g1.chain = chain;
+  g1.tiles_m = mt1;
+  g1.tiles_n = nt1;
+  g1.n_fast = 0;
   g1.terms = terms;
-  if (t0) cudaEventRecord(t0, st);
-  tc::k_gemm_tf32x3<1, 0><<<dim3(mt1, nt1, nsplit), tc::kThreads, tc::kSmemBytes, st>>>(g1);
-  float* b2 = (float*)c->tc_b2.p;
-  tc::k_reduce_p<<<std::max(1, std::min(1184, (na * nb + 255) / 256)), 256, 0, st>>>(
-      na, nb, nsplit, mpad, k2p, (const float*)c->tc_part.p, b2, b2 + (size_t)(2 * nb) * k2p);
-  if (t1) cudaEventRecord(t1, st);
-  // GEMM 2: mtxd x (2 nb), K = 2 nanl, accumulate into hpsi
+  g1.out = (double*)c->tc_part.p;
+  g1.err = (int*)c->tc_err.p;
+
+  // GEMM 2: mtxd x (2 nb), K = 2 nanl, added into hpsi
+  const int mt2 = (m + tc::BM - 1) / tc::BM, nt2 = (2 * nb + tc::BN - 1) / tc::BN;
   tc::GemmArgs g2{};
+  g2.a_hi = a2;
+  g2.a_lo = a2 + fa2;
+  g2.b_hi = b2;
+  g2.b_lo = b2 + fb2;
   g2.M = m;
   g2.N = 2 * nb;
-  g2.K = (int)k2p;
-  g2.kb_per_split = (int)(k2p / tc::BK);
-  g2.a_hi = (const float*)c->tc_a2.p;
-  g2.a_lo = g2.a_hi + (size_t)m * k2p;
-  g2.lda = k2p;
-  g2.b_hi = b2;
-  g2.b_lo = b2 + (size_t)(2 * nb) * k2p;
-  g2.ldb = k2p;
-  g2.hpsi = (double*)hpsi;
-  g2.ldh = ldh;
-  g2.nbh = nb;
-  g2.err = (int*)c->tc_err.p;
+  g2.nkb = (int)nkb2;
+  g2.kb_per_split = (int)nkb2;
+  g2.nsplit = 1;
+  g2.chain = chain;
+  g2.tiles_m = mt2;
+  g2.tiles_n = nt2;
+  g2.n_fast = 1;
   g2.terms = terms;
-  tc::k_gemm_tf32x3<0, 1><<<dim3((m + tc::BM - 1) / tc::BM, (2 * nb + tc::BN - 1) / tc::BN, 1), tc::kThreads,
-                            tc::kSmemBytes, st>>>(g2);
+  g2.out = (double*)hpsi;
+  g2.ldh = ldh;
+  g2.err = (int*)c->tc_err.p;
+
+  cudaError_t e = cudaMemsetAsync(c->tc_err.p, 0, sizeof(int), st);
+  if (e != cudaSuccess) return cuda_fail(e, "tc nl");
+  if ((e = cudaFuncSetAttribute(tc::k_gemm_tf32x3<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                tc::kSmemBytes)) != cudaSuccess ||
+      (e = cudaFuncSetAttribute(tc::k_gemm_tf32x3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                tc::kSmemBytes)) != cudaSuccess)
+    return cuda_fail(e, "tensor-core GEMM attribute");
+  const int items1 = mt1 * nt1 * nsplit, items2 = mt2 * nt2;
+  if (t0) cudaEventRecord(t0, st);
+  tc::k_split_psi<<<grid_for((long long)nb * nkb1 * 16, nsm), 256, 0, st>>>(nb, m, nkb1, (const C2<double>*)psi, ldpsi,
+                                                                             b1, b1 + fb1);
+  tc::k_gemm_tf32x3<0><<<std::min(items1, nsm), tc::kThreads, tc::kSmemBytes, st>>>(g1);
+  if ((2LL * na) % tc::BK) {
+    if ((e = cudaMemsetAsync(b2, 0, sizeof(float) * 2 * fb2, st)) != cudaSuccess) return cuda_fail(e, "tc nl");
+  }
+  tc::k_reduce_p<<<grid_for((long long)na * nb, nsm), 256, 0, st>>>(na, nb, nsplit, nkb2, (const double*)c->tc_part.p,
+                                                                    b2, b2 + fb2);
+  if (t1) cudaEventRecord(t1, st);
+  tc::k_gemm_tf32x3<1><<<std::min(items2, nsm), tc::kThreads, tc::kSmemBytes, st>>>(g2);
   if (t2) cudaEventRecord(t2, st);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "tensor-core projector GEMMs");
   return kOk;

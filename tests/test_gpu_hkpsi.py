@@ -63,7 +63,7 @@ def test_device_fp64_si64_box96(cuda):
     assert relerr(got, oracle_hpsi(d, psi, 6)) < TOL64
 
 
-@pytest.mark.parametrize("prec,tol", [(0, TOL64), (1, TOL32)])
+@pytest.mark.parametrize("prec,tol", [(0, TOL64), (1, TOL32), (2, TOL32)])
 def test_device_box40_kpoint_batch_cell(cuda, prec, tol):
     import torch
     w = configs.si8_cubic_kbatch()
@@ -74,7 +74,7 @@ def test_device_box40_kpoint_batch_cell(cuda, prec, tol):
     assert relerr(got, oracle_hpsi(d, psi, 5)) < tol
 
 
-@pytest.mark.parametrize("prec,tol", [(0, TOL64), (1, TOL32)])
+@pytest.mark.parametrize("prec,tol", [(0, TOL64), (1, TOL32), (2, TOL32)])
 def test_device_box144_si216(cuda, prec, tol):
     import torch
     w = configs.si216_cubic()
@@ -211,3 +211,24 @@ def test_mixed_projector_products_on_tensor_cores(cuda):
         out[prec] = (full - loc - kin).cpu().numpy()       # the projector term
     ref = out[H.FP64]
     assert relerr(out[H.MIXED_TC], ref) < 1.5e-6
+
+
+@pytest.mark.parametrize("wname,nb", [("si2_fcc", 3), ("small_test", 5), ("si8_cubic_kbatch", 17), ("si8_cubic_kbatch", 130)])
+def test_mixed_tc_edge_shapes(cuda, wname, nb):
+    """Tensor-core projector path on shapes with partial 128-row tiles, K not a multiple of 32
+    (2 nanl = 16 and 64), band counts below 16 and just above 128: the projector term agrees with
+    the FP64 path to 1e-7 of its size, the full H|psi> with the oracle to the FP32 tolerance."""
+    import torch
+    w = getattr(configs, wname)()
+    d = configs.kpoint_inputs(w, 1 if wname == "si8_cubic_kbatch" else 0)
+    psi = configs.random_psi(d["mtxd"], nb, 29)
+    nl = {}
+    for prec in (H.FP64, H.MIXED_TC):
+        ctx = H.Context(0, precision=prec).setup(d)
+        full = run_device(ctx, psi, torch, cuda)
+        loc = run_device(ctx, psi, torch, cuda, local_only=True)
+        ctx.synchronize()
+        nl[prec] = full - loc
+        if prec == H.MIXED_TC:
+            assert relerr(full, oracle_hpsi(d, psi, nb)) < TOL32
+    assert relerr(nl[H.MIXED_TC], nl[H.FP64]) < 1e-7
