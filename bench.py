@@ -166,6 +166,90 @@ def time_to_eigvals(d, local, icmax=300, nocc=128):
     return out
 
 
+def run_eig_study(args, local):
+    """Eigensolver to convergence on one workload, FP64 drop-in vs the mixed form, then adjoint forces.
+
+    Prints one JSON line: per variant the iteration trace summary; time-to-eigvals of the mixed form =
+    elapsed time at the first outer iteration whose lowest nocc (occupied) Ritz values are all within
+    1e-6 Ha of the converged FP64 values (FP64: within 1e-8 Ha of its own converged values); and the
+    largest difference between the adjoint forces of the two converged wavefunction sets.
+    """
+    import torch
+
+    from cpw2000_b200 import crystal
+    from cpw2000_b200 import ditsp as E
+    from cpw2000_b200 import forces as FF
+    from cpw2000_b200 import hk_psi as H
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = {"si216": configs.si216_cubic, "si64": configs.si64_cubic, "zb64": configs.zb64_cubic}[args.workload]()
+    nb = {"si216": 480, "si64": 160, "zb64": 160}[args.workload]
+    t0 = time.time()
+    d = configs.kpoint_inputs(w, 0, with_hamsm=True)
+    natom = sum(sp.natom for sp in w.species)
+    nocc = 2 * natom
+    out = {"mode": "eig", "workload": args.workload, "mtxd": d["mtxd"], "nanl": d["nanl"], "bands": nb,
+           "occupied": nocc, "epspsi": args.epspsi, "icmax": args.icmax, "setup_s": time.time() - t0}
+    known = {"fp64": (H.FP64, {}), "fp64_cholqr": (H.FP64, {"CPW_B200_ORTHO": "cholqr"}),
+             "mixed": (H.MIXED, {}), "mixed_tc": (H.MIXED_TC, {})}
+    names = ["fp64"] + [v for v in args.variants.split(",") if v and v != "fp64"]
+    if args.with_cholqr and "fp64_cholqr" not in names:
+        names.insert(1, "fp64_cholqr")
+    variants = [(n, known[n][0], known[n][1]) for n in names]
+    traces, psis = {}, {}
+    for name, prec, env in variants:
+        os.environ.pop("CPW_B200_ORTHO", None)
+        os.environ.update(env)
+        ctx = H.Context(local, precision=prec).setup(d)
+        ctx.set_slab_budget(4 << 30)
+        P = torch.zeros((3 * nb, d["mtxd"]), dtype=torch.complex128, device=dev).t()
+        HP = torch.zeros_like(P)
+        torch.cuda.synchronize()
+        icmax = args.icmax_ref if (name == "fp64" and args.icmax_ref) else args.icmax
+        r = E.eigensolve(ctx, P, HP, nb, d["mtxds"], d["hamsm"], d["hdiag"], epspsi=args.epspsi, icmax=icmax,
+                         trace=True)
+        ctx.close()
+        traces[name] = r["trace"]
+        if args.save_traces:
+            os.makedirs(args.save_traces, exist_ok=True)
+            np.save(os.path.join(args.save_traces, f"trace_{args.workload}_{name}.npy"), r["trace"])
+        psis[name] = P[:, :nocc].clone()
+        out[name] = {"converged": bool(r["converged"]), "outer_iterations": int(r["trace"].shape[0]),
+                     "seconds_total": float(r["trace"][-1, 0]), "hpsi_band_products": int(r["ihkpsum"]),
+                     "xmax_end": float(r["trace"][-1, 1])}
+        del P, HP
+        torch.cuda.empty_cache()
+    os.environ.pop("CPW_B200_ORTHO", None)
+    ref = traces["fp64"][-1, 4:4 + nocc]
+    for name, _, _ in variants:
+        tol = 1e-8 if name.startswith("fp64") else 1e-6
+        err = np.abs(traces[name][:, 4:4 + nocc] - ref[None, :]).max(axis=1)
+        ok = np.nonzero(err <= tol)[0]
+        k = int(ok[0]) if len(ok) else None
+        out[name].update({"tolerance_ha": tol, "seconds_to_tolerance": float(traces[name][k, 0]) if k is not None
+                          else None, "iterations_to_tolerance": k + 1 if k is not None else None,
+                          "max_err_ha_at_end": float(err[-1])})
+    for name in [v[0] for v in variants[1:]]:
+        a, b = out["fp64"]["seconds_to_tolerance"], out[name]["seconds_to_tolerance"]
+        if a and b:
+            out[f"speedup_{name}_vs_fp64"] = a / b
+    # adjoint forces (FP64 adjoint) from the converged occupied wavefunctions of each variant
+    fcart = {}
+    for name in psis:
+        s = FF.HFSystem(w, d, psis[name], np.full(nocc, 2.0), device=local)
+        _, f = FF.forces(s)
+        fcart[name] = FF.to_cartesian(f, w.adot)
+        s.ctx.close()
+    for name in fcart:
+        if name != "fp64":
+            out[name]["force_max_abs_diff_ha_bohr_vs_fp64"] = float(np.abs(fcart[name] - fcart["fp64"]).max())
+    out["force_max_abs_ha_bohr"] = float(np.abs(fcart["fp64"]).max())
+    out["definition"] = (f"time to the lowest {nocc} Ritz values within the tolerance of the FP64 path's converged "
+                         f"values; epspsi {args.epspsi}; start basis from the {d['mtxds']}x{d['mtxds']} small "
+                         "matrix (iguess 0); forces: Hellmann-Feynman via the adjoint, occupation 2 per band")
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -400,7 +484,16 @@ def run_profile(args, local):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--mode", choices=["bench", "profile"], default="bench")
+    ap.add_argument("--mode", choices=["bench", "profile", "eig"], default="bench")
+    ap.add_argument("--workload", choices=["si216", "si64", "zb64"], default="si216", help="eig mode workload")
+    ap.add_argument("--icmax", type=int, default=200, help="eig mode: outer iterations at most")
+    ap.add_argument("--epspsi", type=float, default=1e-5, help="eig mode: residual tolerance")
+    ap.add_argument("--with-cholqr", action="store_true", help="eig mode: also FP64 with Cholesky QR")
+    ap.add_argument("--variants", default="mixed_tc", help="eig mode: comma list of fp64_cholqr, mixed, mixed_tc "
+                    "(fp64 always runs first as the reference)")
+    ap.add_argument("--icmax-ref", type=int, default=0, help="eig mode: outer iterations of the FP64 reference run "
+                    "(default: --icmax)")
+    ap.add_argument("--save-traces", default="", help="eig mode: directory for the iteration traces (.npy)")
     ap.add_argument("--bands", type=int, default=NB, help="profile mode: bands per call")
     ap.add_argument("--precision", choices=["fp64", "mixed", "mixed_tc"], default="fp64", help="profile mode precision")
     ap.add_argument("--gpus", type=int, default=1)
@@ -413,6 +506,8 @@ def main():
     try:
         if args.mode == "profile":
             run_profile(args, local)
+        elif args.mode == "eig":
+            run_eig_study(args, local)
         elif args.impl == "reference":
             run_reference(args, rank)
         else:

@@ -60,6 +60,8 @@ int tc_prepare_projectors(cpw_b200_ctx* c);
 int tc_nl_apply(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh, cudaStream_t st,
                 cudaEvent_t t0, cudaEvent_t t1, cudaEvent_t t2);
 int tc_check_error(cpw_b200_ctx* c);
+int tc_zgemm_nn(cpw_b200_ctx* c, int m, int n, int kk, const void* a, long long lda, const void* b, long long ldb,
+                void* cm, long long ldc, cudaStream_t st);
 int density_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, const double* occ, void* rho,
                    cudaStream_t st);
 int structure_grad_device(cpw_b200_ctx* c, const void* g, int natom, const int* atom_type, const double* tau,
@@ -93,7 +95,7 @@ struct cpw_b200_ctx {
   cpwb::DevBuf anl, anld, proj;
   std::vector<double> xnl_h;    // host copy of xnlkb
   // mixed precision: split-TF32 operands of the tensor-core projector GEMMs
-  cpwb::DevBuf tc_a1, tc_a2, tc_b1, tc_part, tc_b2, tc_err;
+  cpwb::DevBuf tc_a1, tc_a2, tc_b1, tc_part, tc_b2, tc_err, tc_ga, tc_gb;
   long long tc_k1p = 0, tc_k2p = 0;     // K blocks (32 reals) of the projection and expansion operands
   bool tc_ready = false;
 

@@ -30,6 +30,31 @@ template <typename T> __device__ __forceinline__ C2<T> cmulc(C2<T> a, C2<T> b) {
   return mk<T>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
 template <typename T> __device__ __forceinline__ C2<T> scal(C2<T> a, T s) { return mk<T>(a.x * s, a.y * s); }
+// A real constant for products in T. In FP32 the constant is carried as hi + lo and applied
+// with one FMA, so that its rounding leaves no systematic gain: a constant rounded once to
+// FP32 (sqrt(3)/2, sqrt(1/2), cos(2 pi/5), ...) scales every value it touches by the same
+// relative error (up to ~3e-8), a bias the forward/inverse pair of transforms accumulates.
+template <typename T> struct K;
+template <> struct K<double> {
+  double v;
+  __host__ __device__ constexpr K(double c) : v(c) {}
+  __device__ __forceinline__ double mul(double x) const { return x * v; }
+};
+template <> struct K<float> {
+  float h, l;
+  __host__ __device__ constexpr K(double c) : h((float)c), l((float)(c - (double)(float)c)) {}
+  __device__ __forceinline__ float mul(float x) const { return fmaf(x, h, x * l); }
+};
+template <typename T> __device__ __forceinline__ C2<T> kscal(C2<T> a, K<T> k) { return mk<T>(k.mul(a.x), k.mul(a.y)); }
+// a * (c + i s) with split constants
+__device__ __forceinline__ C2<double> kcmul(C2<double> a, K<double> c, K<double> s) {
+  return mk<double>(a.x * c.v - a.y * s.v, a.x * s.v + a.y * c.v);
+}
+__device__ __forceinline__ C2<float> kcmul(C2<float> a, K<float> c, K<float> s) {
+  const float re_lo = a.x * c.l - a.y * s.l, im_lo = a.x * s.l + a.y * c.l;
+  return mk<float>(fmaf(a.x, c.h, fmaf(-a.y, s.h, re_lo)), fmaf(a.x, s.h, fmaf(a.y, c.h, im_lo)));
+}
+
 // multiply by i*S (S = +1 or -1)
 template <int S, typename T> __device__ __forceinline__ C2<T> mul_iS(C2<T> a) {
   return S > 0 ? mk<T>(-a.y, a.x) : mk<T>(a.y, -a.x);
@@ -86,10 +111,10 @@ template <int S, typename T> struct DFT<2, S, T> {
 
 template <int S, typename T> struct DFT<3, S, T> {
   static __device__ __forceinline__ void run(C2<T>* v) {
-    const T h = T(0.866025403784438646763723170752936183);  // sqrt(3)/2
+    constexpr K<T> h(0.866025403784438646763723170752936183);  // sqrt(3)/2
     C2<T> t1 = v[1] + v[2];
     C2<T> t2 = v[0] - scal<T>(t1, T(0.5));
-    C2<T> t3 = mul_iS<S, T>(scal<T>(v[1] - v[2], h));
+    C2<T> t3 = mul_iS<S, T>(kscal<T>(v[1] - v[2], h));
     v[0] = v[0] + t1;
     v[1] = t2 + t3;
     v[2] = t2 - t3;
@@ -106,15 +131,15 @@ template <int S, typename T> struct DFT<4, S, T> {
 
 template <int S, typename T> struct DFT<5, S, T> {
   static __device__ __forceinline__ void run(C2<T>* v) {
-    const T c1 = T(0.309016994374947424102293417182819059);   // cos(2pi/5)
-    const T c2 = T(-0.809016994374947424102293417182819059);  // cos(4pi/5)
-    const T s1 = T(0.951056516295153572116439333379382143);   // sin(2pi/5)
-    const T s2 = T(0.587785252292473129168705954639072769);   // sin(4pi/5)
+    constexpr K<T> c1(0.309016994374947424102293417182819059);   // cos(2pi/5)
+    constexpr K<T> c2(-0.809016994374947424102293417182819059);  // cos(4pi/5)
+    constexpr K<T> s1(0.951056516295153572116439333379382143);   // sin(2pi/5)
+    constexpr K<T> s2(0.587785252292473129168705954639072769);   // sin(4pi/5)
     C2<T> t1 = v[1] + v[4], t2 = v[2] + v[3], t3 = v[1] - v[4], t4 = v[2] - v[3];
-    C2<T> a1 = v[0] + scal<T>(t1, c1) + scal<T>(t2, c2);
-    C2<T> a2 = v[0] + scal<T>(t1, c2) + scal<T>(t2, c1);
-    C2<T> b1 = mul_iS<S, T>(scal<T>(t3, s1) + scal<T>(t4, s2));
-    C2<T> b2 = mul_iS<S, T>(scal<T>(t3, s2) - scal<T>(t4, s1));
+    C2<T> a1 = v[0] + kscal<T>(t1, c1) + kscal<T>(t2, c2);
+    C2<T> a2 = v[0] + kscal<T>(t1, c2) + kscal<T>(t2, c1);
+    C2<T> b1 = mul_iS<S, T>(kscal<T>(t3, s1) + kscal<T>(t4, s2));
+    C2<T> b2 = mul_iS<S, T>(kscal<T>(t3, s2) - kscal<T>(t4, s1));
     v[0] = v[0] + t1 + t2;
     v[1] = a1 + b1; v[4] = a1 - b1;
     v[2] = a2 + b2; v[3] = a2 - b2;
@@ -145,8 +170,7 @@ template <int A, int B, int S, typename T> struct DFTComp {
         } else if (4 * m == 3 * R) {             // W = -i*S
           t[k1 * B + n2] = mul_iS<-S, T>(u[k1]);
         } else {
-          C2<T> w = mk<T>(T(tw.c[m]), T(S * tw.s[m]));
-          t[k1 * B + n2] = cmul<T>(u[k1], w);
+          t[k1 * B + n2] = kcmul(u[k1], K<T>(tw.c[m]), K<T>(S * tw.s[m]));
         }
       }
     }

@@ -9,6 +9,7 @@
 #include <cusolverDn.h>
 #include <math.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -391,6 +392,70 @@ struct Solver {
     return kOk;
   }
 
+  // ---- Cholesky QR, twice: the in-block orthonormalisation of the mixed form ----
+  // X <- X (L^H)^-1 with X^H X = L L^H, two passes. Before the first pass changes X, a
+  // failed factorisation or a pivot L_ii^2 below kCholDrop * xscl_i (near dependence, where
+  // the reference's drop rule may apply) sets *fallback and leaves X to the reference's
+  // recursive Gram-Schmidt.
+  bool chol = false;
+  bool tc_rot = false;   // Ritz rotations on the tensor cores (mixed form with tensor-core projectors)
+  long long n_chol = 0, n_chol_fallback = 0;
+  DevBuf chol_g, chol_work, chol_info;
+  static constexpr double kCholDrop = 1e-12;
+  int cholqr(bool also, Z* x, Z* hx, int k, const double* xscl, bool* fallback) {
+    *fallback = false;
+    if (k <= 0) return kOk;
+    Tick tk(this, 3);
+    ++n_chol;
+    if (!sol) {
+      if (cusolverDnCreate(&sol) != CUSOLVER_STATUS_SUCCESS) return fail(kCusolver, "cusolverDnCreate failed");
+      cusolverDnSetStream(sol, st);
+    }
+    int s;
+    if ((s = chol_g.ensure(sizeof(Z) * (size_t)k * k)) || (s = chol_info.ensure(sizeof(int)))) return s;
+    Z* G = (Z*)chol_g.p;
+    int lw = 0;
+    if (cusolverDnZpotrf_bufferSize(sol, CUBLAS_FILL_MODE_LOWER, k, G, k, &lw) != CUSOLVER_STATUS_SUCCESS)
+      return fail(kCusolver, "zpotrf workspace");
+    if ((s = chol_work.ensure(sizeof(Z) * (size_t)std::max(lw, 1)))) return s;
+    std::vector<Z> dg(k);
+    for (int pass = 0; pass < 2; ++pass) {
+      {
+        const double a1 = 1.0, b0 = 0.0;   // lower triangle of X^H X
+        if (cublasZherk(blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, k, m, &a1, x, m, &b0, G, k) != CUBLAS_STATUS_SUCCESS)
+          return fail(kCublas, "cholqr gram");
+      }
+      if (cusolverDnZpotrf(sol, CUBLAS_FILL_MODE_LOWER, k, G, k, (Z*)chol_work.p, lw, (int*)chol_info.p) !=
+          CUSOLVER_STATUS_SUCCESS)
+        return fail(kCusolver, "zpotrf");
+      int info = 0;
+      if ((s = ck(cudaMemcpyAsync(&info, chol_info.p, sizeof(int), cudaMemcpyDeviceToHost, st), "cholqr info")) ||
+          (s = ck(cudaMemcpy2DAsync(dg.data(), sizeof(Z), G, sizeof(Z) * (size_t)(k + 1), sizeof(Z), k,
+                                    cudaMemcpyDeviceToHost, st),
+                  "cholqr diag")) ||
+          (s = ck(cudaStreamSynchronize(st), "cholqr")))
+        return s;
+      bool bad = info != 0;
+      for (int i = 0; i < k && !bad && pass == 0; ++i)
+        if (!(dg[i].x * dg[i].x > kCholDrop * xscl[i])) bad = true;
+      if (bad) {
+        if (pass == 0) {
+          *fallback = true;
+          ++n_chol_fallback;
+          return kOk;
+        }
+        return fail(kCusolver, "cholqr: second Cholesky pass failed");
+      }
+      if (cublasZtrsm(blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, CUBLAS_DIAG_NON_UNIT, m, k, &one,
+                      G, k, x, m) != CUBLAS_STATUS_SUCCESS)
+        return fail(kCublas, "cholqr trsm");
+      if (also && cublasZtrsm(blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, CUBLAS_DIAG_NON_UNIT, m,
+                              k, &one, G, k, hx, m) != CUBLAS_STATUS_SUCCESS)
+        return fail(kCublas, "cholqr trsm");
+    }
+    return kOk;
+  }
+
   // ---- block Gram-Schmidt family (grsch_mod / grsch_mm / grsch_loop / grsch_shift) ----
   // grsch_mod on the device (k_mgs); irow/xscl are host arrays of nvec entries
   DevBuf mgs_part, mgs_bar, mgs_irow, mgs_xscl;
@@ -511,6 +576,12 @@ struct Solver {
             return s;
       }
     }
+    if (chol) {
+      bool fb = false;
+      if (int s = cholqr(also, x + (size_t)nconv * m, also ? hx + (size_t)nconv * m : nullptr, k, xscl.data(), &fb))
+        return s;
+      if (!fb) return kOk;
+    }
     return grsch_mm(also, x + (size_t)nconv * m, also ? hx + (size_t)nconv * m : nullptr, k, irow.data() + nconv,
                     xscl.data());
   }
@@ -612,6 +683,14 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
   S.P = (Z*)psi;
   S.HP = (Z*)hpsi;
   S.timing = ipr > 1;
+  // in-block orthonormalisation: the reference's recursive Gram-Schmidt for the FP64 drop-in,
+  // Cholesky QR twice for the mixed form; CPW_B200_ORTHO=mgs|cholqr overrides
+  S.chol = c->precision != 0;
+  S.tc_rot = c->precision == 2 && !(getenv("CPW_B200_TC_ROT") && !strcmp(getenv("CPW_B200_TC_ROT"), "0"));
+  if (const char* o = getenv("CPW_B200_ORTHO")) {
+    if (!strcmp(o, "mgs")) S.chol = false;
+    if (!strcmp(o, "cholqr")) S.chol = true;
+  }
   const auto t_start = std::chrono::steady_clock::now();
   int s;
   if ((s = S.eg_d.ensure(sizeof(double) * (size_t)std::max(mxdsml, 1)))) return s;
@@ -957,9 +1036,14 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
     const int lo = nexact + nconv;
     if ((s = S.hk(S.B(lo), mtxd, S.HB(lo), mtxd, nsize - lo))) return s;
     if ((s = S.smallV.ensure(sizeof(Z) * (size_t)nsize * nsize))) return s;
-    if ((s = S.gemm(CUBLAS_OP_C, CUBLAS_OP_N, nsize, nsize, mtxd, S.one, (Z*)S.hbas.p, mtxd, (Z*)S.bas.p, mtxd, S.zero,
-                    (Z*)S.smallV.p, nsize, "ritz hamsm")))
-      return s;
+    // hamsm = hbas^H bas (ditsp_c16_ritz.f90:195); zheevd reads its lower triangle only, which
+    // zherkx computes at half the cost of the full product
+    {
+      const double b0 = 0.0;
+      if (cublasZherkx(S.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, nsize, mtxd, &S.one, (Z*)S.hbas.p, mtxd,
+                       (Z*)S.bas.p, mtxd, &b0, (Z*)S.smallV.p, nsize) != CUBLAS_STATUS_SUCCESS)
+        return fail(kCublas, "ritz hamsm");
+    }
     std::vector<double> egs;
     if ((s = S.diag((Z*)S.smallV.p, nsize, egs))) return s;
     for (int i = 0; i < nsize; ++i) eg[i] = egs[i];
@@ -1009,12 +1093,20 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
         if (ljump || nconv == 0) break;
       }
     }
-    if ((s = S.gemm(CUBLAS_OP_N, CUBLAS_OP_N, mtxd, niter, nsize, S.one, (Z*)S.bas.p, mtxd, (Z*)S.smallV.p, nsize,
-                    S.zero, PP, mtxd, "ritz psi")))
-      return s;
-    if ((s = S.gemm(CUBLAS_OP_N, CUBLAS_OP_N, mtxd, niter, nsize, S.one, (Z*)S.hbas.p, mtxd, (Z*)S.smallV.p, nsize,
-                    S.zero, HPP, mtxd, "ritz hpsi")))
-      return s;
+    // psi = bas V, hpsi = hbas V (ditsp_c16_ritz.f90:284-287): split-TF32 tensor-core products in the
+    // mixed form (V and the subspace Hamiltonian stay FP64), FP64 ZGEMM otherwise
+    if (S.tc_rot) {
+      if ((s = tc_zgemm_nn(c, mtxd, niter, nsize, S.bas.p, mtxd, S.smallV.p, nsize, PP, mtxd, st)) ||
+          (s = tc_zgemm_nn(c, mtxd, niter, nsize, S.hbas.p, mtxd, S.smallV.p, nsize, HPP, mtxd, st)))
+        return s;
+    } else {
+      if ((s = S.gemm(CUBLAS_OP_N, CUBLAS_OP_N, mtxd, niter, nsize, S.one, (Z*)S.bas.p, mtxd, (Z*)S.smallV.p, nsize,
+                      S.zero, PP, mtxd, "ritz psi")))
+        return s;
+      if ((s = S.gemm(CUBLAS_OP_N, CUBLAS_OP_N, mtxd, niter, nsize, S.one, (Z*)S.hbas.p, mtxd, (Z*)S.smallV.p, nsize,
+                      S.zero, HPP, mtxd, "ritz hpsi")))
+        return s;
+    }
     if (niter > nconv) {
       if ((s = S.copycols(S.B(nexact + nconv), mtxd, PP + (size_t)nconv * mtxd, mtxd, niter - nconv))) return s;
       if ((s = S.copycols(S.HB(nexact + nconv), mtxd, HPP + (size_t)nconv * mtxd, mtxd, niter - nconv))) return s;
@@ -1064,8 +1156,8 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
            "subspace eigensolve %.4f s, other %.4f s\n",
            S.ihk, tot, S.tphase[0], S.tphase[1], S.tphase[2], tot - S.tphase[0] - S.tphase[1] - S.tphase[2]);
     printf("  ditsp_c16: Gram-Schmidt %lld calls, %lld vectors: passes against converged %.4f s, "
-           "%lld modified Gram-Schmidt leaves %.4f s\n",
-           S.n_gs, S.n_gs_vec, S.tphase[4], S.n_leaf, S.tphase[3]);
+           "in-block %.4f s (%lld modified Gram-Schmidt leaves, %lld Cholesky QR, %lld fallbacks)\n",
+           S.n_gs, S.n_gs_vec, S.tphase[4], S.tphase[3], S.n_leaf, S.n_chol, S.n_chol_fallback);
     fflush(stdout);
   }
   if (S.sol) cusolverDnDestroy(S.sol);

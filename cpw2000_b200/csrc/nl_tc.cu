@@ -24,17 +24,18 @@
 //   warp 0      producer: bulk copies of A hi/lo and B hi/lo into a 3-stage ring
 //               (full/empty mbarriers);
 //   warp 1      allocates 512 TMEM columns; one lane issues tcgen05.mma kind::tf32
-//               (M 128, K 8): A hi . [B hi; B lo] as one N = 2 n MMA into adjacent
-//               main (hi.hi) and correction (hi.lo) columns, then A lo . B hi into
-//               the correction columns; two such accumulator pairs alternate;
-//   warps 2-9   drain: every `chain` K blocks they read a finished pair with
-//               tcgen05.ld, add main + correction in FP32 and accumulate in FP64
-//               registers (one row and 64 columns per thread), release the pair,
-//               and store the tile after its last chunk.
-// The FP32 accumulation of the tensor cores carries a systematic rounding bias
-// (measured: it grows with the number of accumulation steps into one accumulator);
-// draining every `chain` blocks keeps the steps per FP32 chain at 4 x chain while
-// the K range per work item stays long. Every mbarrier wait is bounded in time: on
+//               (M 128, N <= 128, K 8): hi.hi into one of three rotating main
+//               accumulators, restarted every `chain` K blocks; hi.lo and lo.hi into
+//               a correction accumulator that spans the whole work item;
+//   warps 2-9   drain: they read each finished main accumulator with tcgen05.ld and
+//               add it into FP64 sums in registers (one row and 64 columns per
+//               thread), release it, add the correction accumulator at the end of
+//               the work item, and store the tile.
+// The FP32 accumulation of the tensor cores shrinks a sum by a fixed fraction per
+// accumulation step (measured: ~5e-7 relative on coherent sums over 16 steps), a
+// bias, not noise. Restarting the hi.hi accumulator every K block (4 steps) keeps it
+// near 1e-7; the correction terms are 2^-11 of the total, so their long chain adds
+// nothing visible; the drain sums in FP64. Every mbarrier wait is bounded in time: on
 // timeout the kernel sets an error flag, skips its stores, waits (bounded) for its
 // copies and MMAs in flight, frees its TMEM and returns.
 #include <stdint.h>
@@ -59,7 +60,8 @@ constexpr int kPrefetch = 8;                       // K blocks fetched into L2 a
 constexpr int kEpiBytes = 2048;                    // per drain warp: 4 complex columns x 32 rows of FP64 staging
 constexpr int kSmemBytes = kStages * kStageBytes + 1024 + kBarBytes + kDrainWarps * kEpiBytes;
 constexpr unsigned long long kWaitNs = 2000000000ull;   // 2 s per mbarrier wait at most
-constexpr int kTmemCols = 512;                     // 2 x (main 128 + correction 128)
+constexpr int kMainBufs = 3;                       // rotating hi.hi accumulators
+constexpr int kTmemCols = 512;                     // correction 128 + 3 x hi.hi 128 (+128 unused)
 
 // float offset of element (r, k) of a tiled operand with nkb K blocks
 __host__ __device__ __forceinline__ size_t tiled_off(long long r, long long k, long long nkb) {
@@ -225,9 +227,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
   uint64_t* bars = reinterpret_cast<uint64_t*>(tiles + kStages * kStageBytes);
   uint64_t* full = bars;                     // [kStages] copies landed
   uint64_t* empty = bars + kStages;          // [kStages] MMAs that read the stage are done
-  uint64_t* accf = bars + 2 * kStages;       // [2] accumulator pair ready for the drain
-  uint64_t* acce = accf + 2;                 // [2] accumulator pair drained
-  uint64_t* done = acce + 2;                 // all MMAs of this CTA complete
+  uint64_t* accf = bars + 2 * kStages;       // [kMainBufs] hi.hi accumulator ready for the drain
+  uint64_t* acce = accf + kMainBufs;         // [kMainBufs] hi.hi accumulator drained
+  uint64_t* corre = acce + kMainBufs;        // correction accumulator drained (end of a work item)
+  uint64_t* done = corre + 1;                // all MMAs of this CTA complete
   uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
   unsigned char* epi = tiles + kStages * kStageBytes + kBarBytes;   // drain-warp staging (mode 1)
   __shared__ volatile int failed;
@@ -242,10 +245,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
       mbar_init(smem_u32(&full[s]), 1);
       mbar_init(smem_u32(&empty[s]), 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < kMainBufs; ++b) {
       mbar_init(smem_u32(&accf[b]), 1);
       mbar_init(smem_u32(&acce[b]), kDrainWarps);
     }
+    mbar_init(smem_u32(corre), kDrainWarps);
     mbar_init(smem_u32(done), 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -292,9 +296,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
           const size_t o = (size_t)(w.kb0 + i) * kTileFloats;
           bulk_load(smem_u32(st), ah + o, bytes_a, fb);
           bulk_load(smem_u32(st + kTileBytes), al + o, bytes_a, fb);
-          // B lo rows follow the n_mma B hi rows: one N = 2 n_mma MMA reads [B hi; B lo]
           bulk_load(smem_u32(st + 2 * kTileBytes), bh + o, bytes_b, fb);
-          bulk_load(smem_u32(st + 2 * kTileBytes + w.n_mma * 128), bl + o, bytes_b, fb);
+          bulk_load(smem_u32(st + 3 * kTileBytes), bl + o, bytes_b, fb);
         }
       }
       // copies still in flight land before the CTA may exit
@@ -305,20 +308,29 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
     if (lane == 0) {
       long long gk = 0;                      // K blocks consumed
       long long gq = 0;                      // accumulation chunks issued
-      for (int it = blockIdx.x; it < nitems && !failed; it += gridDim.x) {
+      int nit = 0;                           // work items of this CTA so far
+      const uint32_t tcorr = tmem;           // columns [0, 128): hi.lo + lo.hi of the whole work item
+      for (int it = blockIdx.x; it < nitems && !failed; it += gridDim.x, ++nit) {
         const Item w = item_of(g, it);
-        const uint32_t idesc = instr_desc(w.n_mma), idesc2 = instr_desc(2 * w.n_mma);
+        const uint32_t idesc = instr_desc(w.n_mma);
         const int nchunk = (w.nblk + chain - 1) / chain;
+        // the previous work item's correction accumulator must have been read
+        if (nit > 0 && !mbar_wait(smem_u32(corre), (uint32_t)((nit - 1) & 1), &failed)) {
+          failed = 1;
+          atomicExch(g.err, 1);
+          break;
+        }
         for (int q = 0; q < nchunk && !failed; ++q, ++gq) {
-          const int b = (int)(gq & 1);
-          if (gq >= 2 && !mbar_wait(smem_u32(&acce[b]), (uint32_t)(((gq >> 1) - 1) & 1), &failed)) {
+          const int b = (int)(gq % kMainBufs);
+          if (gq >= kMainBufs &&
+              !mbar_wait(smem_u32(&acce[b]), (uint32_t)((gq / kMainBufs - 1) & 1), &failed)) {
             failed = 1;
             atomicExch(g.err, 1);
             break;
           }
           asm volatile("tcgen05.fence::after_thread_sync;\n");
-          // buffer b: columns [b*256, +n_mma) hi.hi, [b*256 + n_mma, +n_mma) hi.lo + lo.hi
-          const uint32_t tmain = tmem + (uint32_t)(b * 2 * BN), tcorr = tmain + (uint32_t)w.n_mma;
+          // hi.hi accumulator b: columns [128 (b + 1), +n_mma)
+          const uint32_t tmain = tmem + (uint32_t)((b + 1) * BN);
           const int i0 = q * chain, i1 = min(w.nblk, i0 + chain);
           bool ok = true;
           for (int i = i0; i < i1; ++i, ++gk) {
@@ -330,13 +342,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
             asm volatile("tcgen05.fence::after_thread_sync;\n");
             unsigned char* st = tiles + s * kStageBytes;
             const uint32_t ah = smem_u32(st), al = smem_u32(st + kTileBytes);
-            const uint32_t bh = smem_u32(st + 2 * kTileBytes), bl = bh + (uint32_t)w.n_mma * 128u;
+            const uint32_t bh = smem_u32(st + 2 * kTileBytes), bl = smem_u32(st + 3 * kTileBytes);
 #pragma unroll
             for (int ks = 0; ks < BK / 8; ++ks) {
               const uint32_t off = ks * 32;     // 8 tf32 = 32 bytes along K inside the swizzled row
               const uint32_t acc = (i == i0 && ks == 0) ? 0u : 1u;
-              mma_tf32(tmain, smem_desc(ah + off), smem_desc(bh + off), idesc2, acc);   // A hi . [B hi; B lo]
-              mma_tf32(tcorr, smem_desc(al + off), smem_desc(bh + off), idesc, 1u);     // A lo . B hi
+              const uint32_t accc = (i == 0 && ks == 0) ? 0u : 1u;
+              mma_tf32(tmain, smem_desc(ah + off), smem_desc(bh + off), idesc, acc);    // hi.hi
+              mma_tf32(tcorr, smem_desc(ah + off), smem_desc(bl + off), idesc, accc);   // hi.lo
+              mma_tf32(tcorr, smem_desc(al + off), smem_desc(bh + off), idesc, 1u);     // lo.hi
               if (g.terms > 3) mma_tf32(tcorr, smem_desc(al + off), smem_desc(bl + off), idesc, 1u);
             }
             mma_commit(smem_u32(&empty[s]));
@@ -365,31 +379,36 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
       for (int j = 0; j < 64; ++j) acc[j] = 0.0;
       bool ok = true;
       for (int q = 0; q < nchunk; ++q, ++gq) {
-        const int b = (int)(gq & 1);
-        if (!mbar_wait(smem_u32(&accf[b]), (uint32_t)((gq >> 1) & 1), &failed)) {
+        const int b = (int)(gq % kMainBufs);
+        if (!mbar_wait(smem_u32(&accf[b]), (uint32_t)((gq / kMainBufs) & 1), &failed)) {
           ok = false;
           failed = 1;
           atomicExch(g.err, 1);
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;\n");
+        const bool last = q == nchunk - 1;
+        // the last chunk's commit also covers every correction MMA of the item: drain it too
+        for (int pass = 0; pass < (last ? 2 : 1); ++pass) {
+          const uint32_t col0 = pass == 0 ? (uint32_t)((b + 1) * BN) : 0u;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const int col = 64 * half + 8 * j;
-          if (col < w.n_mma) {          // n_mma is a multiple of 16: whole 8-column pieces
-            uint32_t rm[8], rc[8];
-            tmem_ld8(lane_base + (uint32_t)(b * 2 * BN + col), rm);
-            tmem_ld8(lane_base + (uint32_t)(b * 2 * BN + w.n_mma + col), rc);
-            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+          for (int j = 0; j < 8; ++j) {
+            const int col = 64 * half + 8 * j;
+            if (col < w.n_mma) {        // n_mma is a multiple of 16: whole 8-column pieces
+              uint32_t r[8];
+              tmem_ld8(lane_base + col0 + (uint32_t)col, r);
+              asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-            for (int t = 0; t < 8; ++t) acc[8 * j + t] += (double)(__uint_as_float(rm[t]) + __uint_as_float(rc[t]));
+              for (int t = 0; t < 8; ++t) acc[8 * j + t] += (double)__uint_as_float(r[t]);
+            }
           }
+          asm volatile("tcgen05.fence::before_thread_sync;\n");
+          __syncwarp();
+          if (lane == 0) mbar_arrive(smem_u32(pass == 0 ? &acce[b] : corre));
         }
-        asm volatile("tcgen05.fence::before_thread_sync;\n");
-        __syncwarp();
-        if (lane == 0) mbar_arrive(smem_u32(&acce[b]));
       }
       if (!ok || failed) break;
+#define CPWB_ACC(j) (acc[j])
       const int m = w.m0 + 32 * quarter + lane;
       if (nchunk > 0 && w.m0 + 32 * quarter < g.M) {      // warp-uniform: the warp has valid rows
 #pragma unroll
@@ -400,7 +419,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
 #pragma unroll
               for (int t = 0; t < 16; ++t) {
                 const int n = w.n0 + col + t;
-                if (n < g.N && m < g.M) g.out[((size_t)w.split * g.N + n) * g.M + m] = acc[16 * j + t];
+                if (n < g.N && m < g.M) g.out[((size_t)w.split * g.N + n) * g.M + m] = CPWB_ACC(16 * j + t);
               }
             } else {
               // four complex columns at a time through this warp's staging slot: [column][32 rows] of
@@ -415,7 +434,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
                 __syncwarp();
 #pragma unroll
                 for (int t = 0; t < 4; ++t)
-                  slot[t * 32 + lane] = make_double2(acc[16 * j + 8 * hh + 2 * t], acc[16 * j + 8 * hh + 2 * t + 1]);
+                  slot[t * 32 + lane] = make_double2(CPWB_ACC(16 * j + 8 * hh + 2 * t), CPWB_ACC(16 * j + 8 * hh + 2 * t + 1));
                 asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
                 __syncwarp();
                 if (lane == 0) {
@@ -432,6 +451,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
       }
     }
   }
+#undef CPWB_ACC
   if (MODE == 1 && warp >= 2 && lane == 0) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;\n");
   __syncthreads();
@@ -496,6 +516,55 @@ __global__ void k_prep_a2(int mtxd, int nanl, long long nkb, const C2<double>* _
       }
     }
     put_split(hi, lo, tiled_off(i, k, nkb), v[0], v[1]);
+  }
+}
+
+// A (m rows, K = 2 kk, tiled) from a complex128 column-major matrix a (ld lda): row i = (re a(i, :), im a(i, :))
+__global__ void k_prep_arows(int m, int kk, long long lda, long long nkb, const C2<double>* __restrict__ a,
+                             float* __restrict__ hi, float* __restrict__ lo) {
+  const long long pairs = nkb * 16;
+  const long long n = (long long)m * pairs;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    // consecutive threads take consecutive rows i (coalesced reads down a column)
+    const long long i = t % m, k = 2 * (t / m);
+    double v[2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const long long kk2 = k + e;
+      v[e] = 0.0;
+      if (kk2 < 2LL * kk) {
+        const long long l = kk2 % kk;
+        const C2<double> z = a[(size_t)l * lda + i];
+        v[e] = kk2 < kk ? z.x : z.y;
+      }
+    }
+    put_split(hi, lo, tiled_off(i, k, nkb), v[0], v[1]);
+  }
+}
+
+// B (2 n rows, K = 2 kk, tiled) from a complex128 kk x n matrix b (ld ldb):
+// row 2j = (re b(:, j), -im b(:, j)), row 2j+1 = (im b(:, j), re b(:, j))
+__global__ void k_prep_bcols(int kk, int n, long long ldb, long long nkb, const C2<double>* __restrict__ b,
+                             float* __restrict__ hi, float* __restrict__ lo) {
+  const long long kpad = nkb * 32;
+  const long long total = (long long)n * kpad;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const long long j = t / kpad, k = t - j * kpad;
+    double ev = 0.0, od = 0.0;
+    if (k < 2LL * kk) {
+      const long long l = k % kk;
+      const C2<double> z = b[(size_t)j * ldb + l];
+      ev = k < kk ? z.x : -z.y;
+      od = k < kk ? z.y : z.x;
+    }
+    auto put = [&](long long row, double v) {
+      const float h = tf32((float)v);
+      const size_t o = tiled_off(row, k, nkb);
+      hi[o] = h;
+      lo[o] = tf32((float)(v - (double)h));
+    };
+    put(2 * j, ev);
+    put(2 * j + 1, od);
   }
 }
 
@@ -578,7 +647,7 @@ int tc_nl_apply(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void*
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const int chain = std::max(1, env_int("CPW_B200_TC_CHAIN", 4));
+  const int chain = std::max(1, env_int("CPW_B200_TC_CHAIN", 1));
   const int terms = env_int("CPW_B200_TC_TERMS", 3) == 4 ? 4 : 3;
 
   // GEMM 1: (2 nanl) x nb, K = 2 mtxd, split over K so that the work items fill the SMs about once
@@ -659,6 +728,55 @@ int tc_nl_apply(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void*
   tc::k_gemm_tf32x3<1><<<std::min(items2, nsm), tc::kThreads, tc::kSmemBytes, st>>>(g2);
   if (t2) cudaEventRecord(t2, st);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "tensor-core projector GEMMs");
+  return kOk;
+}
+
+// C (m x n) = A (m x kk) B (kk x n), complex128 column-major, in split TF32 on the tensor cores
+int tc_zgemm_nn(cpw_b200_ctx* c, int m, int n, int kk, const void* a, long long lda, const void* b, long long ldb,
+                void* cm, long long ldc, cudaStream_t st) {
+  if (m <= 0 || n <= 0) return kOk;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaError_t e = cudaMemset2DAsync(cm, sizeof(C2<double>) * (size_t)ldc, 0, sizeof(C2<double>) * (size_t)m, n, st);
+  if (e != cudaSuccess) return cuda_fail(e, "tc zgemm");
+  if (kk <= 0) return kOk;
+  const long long nkb = (2LL * kk + tc::BK - 1) / tc::BK;
+  const size_t fa = tc::tiled_floats(m, nkb), fb = tc::tiled_floats(2LL * n, nkb);
+  int s;
+  if ((s = c->tc_ga.ensure(sizeof(float) * 2 * fa)) || (s = c->tc_gb.ensure(sizeof(float) * 2 * fb)) ||
+      (s = c->tc_err.ensure(sizeof(int))))
+    return s;
+  float* ga = (float*)c->tc_ga.p;
+  float* gb = (float*)c->tc_gb.p;
+  tc::k_prep_arows<<<grid_for((long long)m * nkb * 16, nsm), 256, 0, st>>>(m, kk, lda, nkb, (const C2<double>*)a, ga,
+                                                                           ga + fa);
+  tc::k_prep_bcols<<<grid_for((long long)n * nkb * 32, nsm), 256, 0, st>>>(kk, n, ldb, nkb, (const C2<double>*)b, gb,
+                                                                           gb + fb);
+  const int mt = (m + tc::BM - 1) / tc::BM, nt = (2 * n + tc::BN - 1) / tc::BN;
+  tc::GemmArgs g{};
+  g.a_hi = ga;
+  g.a_lo = ga + fa;
+  g.b_hi = gb;
+  g.b_lo = gb + fb;
+  g.M = m;
+  g.N = 2 * n;
+  g.nkb = (int)nkb;
+  g.kb_per_split = (int)nkb;
+  g.nsplit = 1;
+  g.chain = std::max(1, env_int("CPW_B200_TC_CHAIN", 1));
+  g.tiles_m = mt;
+  g.tiles_n = nt;
+  g.n_fast = 1;
+  g.terms = 3;
+  g.out = (double*)cm;
+  g.ldh = ldc;
+  g.err = (int*)c->tc_err.p;
+  if ((e = cudaFuncSetAttribute(tc::k_gemm_tf32x3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                tc::kSmemBytes)) != cudaSuccess)
+    return cuda_fail(e, "tensor-core GEMM attribute");
+  tc::k_gemm_tf32x3<1><<<std::min(mt * nt, nsm), tc::kThreads, tc::kSmemBytes, st>>>(g);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "tensor-core zgemm");
   return kOk;
 }
 

@@ -62,13 +62,31 @@ def test_ditsp_fp64_matches_dense_truth_and_oracle(cuda, ik):
     assert abs(ro["ihkpsum"] - r["ihkpsum"]) <= 0.1 * ro["ihkpsum"]
 
 
-def test_ditsp_mixed_within_1e6(cuda):
+@pytest.mark.parametrize("prec", [H.MIXED, H.MIXED_TC])
+def test_ditsp_mixed_within_1e6(cuda, prec):
+    """Mixed form (FP32 local part; MIXED_TC also split-TF32 projector products and Ritz rotations;
+    both with Cholesky QR in-block orthonormalisation) within 1e-6 Ha of dense truth."""
     import torch
     w = configs.si2_fcc()
     d = configs.kpoint_inputs(w, 2, with_hamsm=True)
-    r, _, _ = device_solve(d, 8, 1e-5, H.MIXED, torch, cuda)
+    r, psi, hpsi = device_solve(d, 8, 1e-5, prec, torch, cuda)
+    assert r["converged"]
     ev = dense_eigs(d)
     assert np.abs(r["ei"] - ev[: r["neig"]]).max() < 1e-6
+    assert D.ditsp_error(psi[:, : r["neig"]], hpsi[:, : r["neig"]]) < 1e-10
+
+
+def test_ditsp_fp64_with_cholesky_qr(cuda, monkeypatch):
+    """The Cholesky QR in-block orthonormalisation on the FP64 path reaches the same eigenvalues
+    (1e-8 Ha of dense truth) as the reference's recursive Gram-Schmidt."""
+    import torch
+    monkeypatch.setenv("CPW_B200_ORTHO", "cholqr")
+    w = configs.si2_fcc()
+    d = configs.kpoint_inputs(w, 4, with_hamsm=True)
+    r, psi, hpsi = device_solve(d, 8, 1e-5, H.FP64, torch, cuda)
+    assert r["converged"] and r["ifail"] == 0
+    assert np.abs(r["ei"] - dense_eigs(d)[: r["neig"]]).max() < 1e-8
+    assert D.ditsp_error(psi[:, : r["neig"]], hpsi[:, : r["neig"]]) < 1e-10
 
 
 def test_ditsp_with_guess_vectors(cuda):
