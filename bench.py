@@ -166,6 +166,60 @@ def time_to_eigvals(d, local, icmax=300, nocc=128):
     return out
 
 
+def kbatch_throughput(local, steps, warmup, nk=64):
+    """Batched H|psi> over the 64 random k-points of the Si8 cubic cell (Ecut 20 Ha, 40^3 box,
+    ~4,600 plane waves per k, 40 bands per k): one batched call (autotuned, replayed from a
+    CUDA graph) per step, against the same work as one H|psi> call per k-point on per-k
+    contexts. Inputs (188 MB of psi and as much hpsi) exceed L2, so no flush between steps."""
+    import torch
+
+    from cpw2000_b200 import hk_psi as H
+    from cpw2000_b200.kbatch import KBatch
+    dev = torch.device("cuda", local)
+    w = configs.si8_cubic_kbatch()
+    inputs = [configs.kpoint_inputs(w, ik) for ik in range(nk)]
+    nbk = 40
+    psis = [torch.from_numpy(np.ascontiguousarray(configs.random_psi(d["mtxd"], nbk, 500 + k).T)).to(dev).t()
+            for k, d in enumerate(inputs)]
+    hps = [torch.empty_like(x) for x in psis]
+    out = {"workload": f"si8 cubic, Ecut 20 Ha, 40^3 box, {nk} random k-points, {nbk} bands per k",
+           "mtxd_min": min(d["mtxd"] for d in inputs), "mtxd_max": max(d["mtxd"] for d in inputs)}
+
+    def timeit(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / steps
+
+    for name, prec in (("fp64", H.FP64), ("mixed_tc", H.MIXED_TC)):
+        ctx = H.Context(local, precision=prec).setup(inputs[0])
+        kb = KBatch(ctx, inputs)
+        kb.hk_psi(psis, hps)                  # autotune + capture
+        ms_b = timeit(lambda: kb.hk_psi(psis, hps))
+        kb.synchronize()
+        info = kb.info()
+        ctxs = [H.Context(local, precision=prec).setup(d) for d in inputs]
+
+        def seq():
+            for c, x, y in zip(ctxs, psis, hps):
+                c.hk_psi(x, y)
+        ms_s = timeit(seq)
+        for c in ctxs:
+            c.close()
+        kb.close()
+        ctx.close()
+        out[name] = {"batched_bands_per_s": nk * nbk / (ms_b / 1e3), "batched_ms": ms_b,
+                     "per_k_loop_bands_per_s": nk * nbk / (ms_s / 1e3), "per_k_loop_ms": ms_s,
+                     "speedup_batched_vs_loop": ms_s / ms_b, "tuning": info}
+    return out
+
+
 def run_eig_study(args, local):
     """Eigensolver to convergence on one workload, FP64 drop-in vs the mixed form, then adjoint forces.
 
@@ -452,6 +506,7 @@ def run_ours(args, world, rank, local, dist):
         "library_launches": {"cublas_zgemm": int(st64["nl_proj"][1] + st64["nl_expand"][1])},
         "clocks": clocks,
     }
+    line["kbatch"] = kbatch_throughput(local, max(3, args.steps // 2), 2)
     if args.eig:
         line["time_to_eigvals"] = time_to_eigvals(d, local)
     if rank == 0 and world == 1:

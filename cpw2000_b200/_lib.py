@@ -42,6 +42,12 @@ SIGNATURES = {
     "cpw_b200_hk_psi_nl_c16": (I, [IP, IP, DP, DP, DP, DP, IP, IP, IP, IP, IP]),
     "hk_psi_nl_c16_": (None, [IP, IP, DP, DP, DP, DP, IP, IP, IP, IP, IP]),
     "cpw_b200_hk_psi_loc_noalloc": (I, [I, I, P, LL, P, LL, P, P, P, IP, P]),
+    "cpw_b200_kbatch_create": (I, [P, I, IP, C.POINTER(IP), IP, I, C.POINTER(DP), IP, C.POINTER(P)]),
+    "cpw_b200_kbatch_destroy": (I, [P]),
+    "cpw_b200_kbatch_set_projectors": (I, [P, I, I, P, LL, DP]),
+    "cpw_b200_kbatch_hk_psi_device": (I, [P, IP, C.POINTER(P), C.POINTER(LL), C.POINTER(P), C.POINTER(LL), P]),
+    "cpw_b200_kbatch_synchronize": (I, [P]),
+    "cpw_b200_kbatch_info": (I, [P, C.POINTER(LL), I]),
     "cpw_b200_density_device": (I, [P, I, P, LL, DP, P, P]),
     "cpw_b200_structure_grad_device": (I, [P, P, I, IP, DP, I, P, DP, P]),
     "cpw_b200_nl_grad_device": (I, [P, I, P, LL, DP, IP, I, DP, P]),

@@ -85,10 +85,13 @@ static void twiddles(int n, std::vector<double>& out) {
   }
 }
 
-static int upload(DevBuf& b, const void* h, size_t bytes) {
+// host -> device copy that has landed when it returns (a pageable cudaMemcpy may return
+// before its DMA completes; work on non-blocking streams must not see a partial copy)
+int upload(DevBuf& b, const void* h, size_t bytes) {
   int s = b.ensure(bytes);
   if (s) return s;
   cudaError_t e = cudaMemcpy(b.p, h, bytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
   return e == cudaSuccess ? kOk : cuda_fail(e, "cudaMemcpy H2D");
 }
 
@@ -98,29 +101,12 @@ static size_t max_smem_optin(int dev) {
   return (size_t)v;
 }
 
-int ctx_set_basis(cpw_b200_ctx* c, int mtxd, const int* isort, const int* kgv, int ng, const double* ekpg,
-                  const int* kmscr) {
-  if (mtxd < 0 || ng < 0) return fail(kBadArg, "set_basis: negative mtxd or ng");
+int plan_for_box(cpw_b200_ctx* c, const int kd[3], const int* kmscr, LocalPlan* out) {
   const int n1 = kmscr[3], n2 = kmscr[4], n3 = kmscr[5];
-  if (n1 < 2 || n2 < 2 || n3 < 2) return fail(kBadArg, "set_basis: FFT dimension less than 2");
-  if (n1 > 65535 || n2 > 65535 || n3 > 65535) return fail(kUnsupported, "set_basis: FFT dimension too large");
-  if (kmscr[6] < n1) return fail(kBadArg, "set_basis: leading dimension kmscr(7) smaller than n1");
   LocalPlan p{};
   p.n1 = n1; p.n2 = n2; p.n3 = n3;
   if (!factor(n1, p.dx) || !factor(n2, p.dy) || !factor(n3, p.dz))
     return fail(kUnsupported, "set_basis: FFT length is not a product of two radices in {1..6,8,9,10,12,16} (max 256)");
-  // sphere extent and wraparound check (hk_psi_c16.f90:145-172)
-  int kd[3] = {0, 0, 0};
-  std::vector<int> g(3 * (size_t)mtxd);
-  for (int i = 0; i < mtxd; ++i) {
-    const int it = isort[i];
-    if (it < 1 || it > ng) return fail(kBadArg, "set_basis: isort out of range of kgv");
-    for (int j = 0; j < 3; ++j) {
-      const int k = kgv[3 * (size_t)(it - 1) + j];
-      g[3 * (size_t)i + j] = k;
-      kd[j] = std::max(kd[j], std::abs(k));
-    }
-  }
   if (kd[0] > (n1 - 1) / 2 || kd[1] > (n2 - 1) / 2 || kd[2] > (n3 - 1) / 2) {
     char buf[256];
     snprintf(buf, sizeof buf, "hk_psi_c16: dimension of k index= %d %d %d exceeds %d %d %d", kd[0], kd[1], kd[2],
@@ -139,9 +125,16 @@ int ctx_set_basis(cpw_b200_ctx* c, int mtxd, const int* isort, const int* kgv, i
     return fail(kUnsupported, "set_basis: plane does not fit in shared memory");
   p.cb = 32;
   while (p.cb > 4 && esz * ((size_t)n3 * p.cb + n3) > cmax) p.cb /= 2;
+  *out = p;
+  return kOk;
+}
+
+void plane_lists(const LocalPlan& p, int mtxd, const int* g, std::vector<int>& start, std::vector<int>& idx,
+                 std::vector<int>& pos) {
+  const int n1 = p.n1, n2 = p.n2, n3 = p.n3;
   // plane lists: basis sorted by kept z-plane
-  std::vector<int> zi(mtxd), order(mtxd);
-  std::vector<int> start(p.nz + 1, 0);
+  std::vector<int> zi(mtxd);
+  start.assign(p.nz + 1, 0);
   for (int i = 0; i < mtxd; ++i) {
     int k3 = g[3 * (size_t)i + 2];
     if (k3 < 0) k3 += n3;
@@ -150,7 +143,8 @@ int ctx_set_basis(cpw_b200_ctx* c, int mtxd, const int* isort, const int* kgv, i
   }
   for (int z = 0; z < p.nz; ++z) start[z + 1] += start[z];
   std::vector<int> fillp(start.begin(), start.end() - 1);
-  std::vector<int> idx(mtxd), pos(mtxd);
+  idx.assign(mtxd, 0);
+  pos.assign(mtxd, 0);
   for (int i = 0; i < mtxd; ++i) {
     int k1 = g[3 * (size_t)i], k2 = g[3 * (size_t)i + 1];
     if (k1 < 0) k1 += n1;
@@ -160,6 +154,31 @@ int ctx_set_basis(cpw_b200_ctx* c, int mtxd, const int* isort, const int* kgv, i
     idx[e] = i;
     pos[e] = (yi << 16) | k1;
   }
+}
+
+int ctx_set_basis(cpw_b200_ctx* c, int mtxd, const int* isort, const int* kgv, int ng, const double* ekpg,
+                  const int* kmscr) {
+  if (mtxd < 0 || ng < 0) return fail(kBadArg, "set_basis: negative mtxd or ng");
+  const int n1 = kmscr[3], n2 = kmscr[4], n3 = kmscr[5];
+  if (n1 < 2 || n2 < 2 || n3 < 2) return fail(kBadArg, "set_basis: FFT dimension less than 2");
+  if (n1 > 65535 || n2 > 65535 || n3 > 65535) return fail(kUnsupported, "set_basis: FFT dimension too large");
+  if (kmscr[6] < n1) return fail(kBadArg, "set_basis: leading dimension kmscr(7) smaller than n1");
+  // sphere extent and wraparound check (hk_psi_c16.f90:145-172)
+  int kd[3] = {0, 0, 0};
+  std::vector<int> g(3 * (size_t)mtxd);
+  for (int i = 0; i < mtxd; ++i) {
+    const int it = isort[i];
+    if (it < 1 || it > ng) return fail(kBadArg, "set_basis: isort out of range of kgv");
+    for (int j = 0; j < 3; ++j) {
+      const int k = kgv[3 * (size_t)(it - 1) + j];
+      g[3 * (size_t)i + j] = k;
+      kd[j] = std::max(kd[j], std::abs(k));
+    }
+  }
+  LocalPlan p{};
+  if (int s = plan_for_box(c, kd, kmscr, &p)) return s;
+  std::vector<int> start, idx, pos;
+  plane_lists(p, mtxd, g.data(), start, idx, pos);
   int s;
   if ((s = upload(c->plane_start, start.data(), start.size() * sizeof(int)))) return s;
   if (mtxd > 0) {

@@ -56,7 +56,24 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
                  void* psi, long long ldp, void* hpsi, const double* hamsm, int mxdsml, const double* hdiag,
                  int mxdbnd, double* ei, long long* ihkpsum, cudaStream_t st, double* itlog = nullptr,
                  int itlog_rows = 0);
+// the local plan of a box for sphere half-widths kd (checks the radix split and the wraparound)
+int plan_for_box(cpw_b200_ctx* c, const int kd[3], const int* kmscr, LocalPlan* out);
+// the kept-plane lists of a basis (g: 3 x mtxd integer G vectors) on plan p
+void plane_lists(const LocalPlan& p, int mtxd, const int* g, std::vector<int>& start, std::vector<int>& idx,
+                 std::vector<int>& pos);
+int upload(DevBuf& b, const void* h, size_t bytes);
+// per-call scratch of the tensor-core projector products and their sticky error flag
+struct TcScratch {
+  DevBuf b1, part, b2, err;
+};
+int tc_error_flag(TcScratch& t);
+int tc_read_error(TcScratch& t);
 int tc_prepare_projectors(cpw_b200_ctx* c);
+int tc_prepare_operands(int m, int na, const void* anl, const void* anld, DevBuf& a1buf, DevBuf& a2buf,
+                        long long* nkb1_out, long long* nkb2_out, cudaStream_t st);
+int tc_nl_apply_ops(TcScratch& t, int m, int na, long long nkb1, long long nkb2, const float* a1, const float* a2,
+                    int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh, cudaStream_t st,
+                    cudaEvent_t t0, cudaEvent_t t1, cudaEvent_t t2, int splits = 0);
 int tc_nl_apply(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh, cudaStream_t st,
                 cudaEvent_t t0, cudaEvent_t t1, cudaEvent_t t2);
 int tc_check_error(cpw_b200_ctx* c);
@@ -95,7 +112,8 @@ struct cpw_b200_ctx {
   cpwb::DevBuf anl, anld, proj;
   std::vector<double> xnl_h;    // host copy of xnlkb
   // mixed precision: split-TF32 operands of the tensor-core projector GEMMs
-  cpwb::DevBuf tc_a1, tc_a2, tc_b1, tc_part, tc_b2, tc_err, tc_ga, tc_gb;
+  cpwb::DevBuf tc_a1, tc_a2, tc_ga, tc_gb;
+  cpwb::TcScratch tcs;
   long long tc_k1p = 0, tc_k2p = 0;     // K blocks (32 reals) of the projection and expansion operands
   bool tc_ready = false;
 

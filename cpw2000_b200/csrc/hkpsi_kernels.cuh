@@ -46,6 +46,14 @@ k_inv_xy(LocalPlan p, int band0, const C2<double>* __restrict__ psi, long long l
   __syncthreads();
 
   const C2<double>* ps = psi + (size_t)(band0 + b) * ldpsi;
+  if (p.kdesc) {      // batch of k-points: this band's own basis and block
+    const int2 r = p.bref[band0 + b];
+    const KDesc& D = p.kdesc[r.x];
+    ps = D.psi + (size_t)r.y * D.ldpsi;
+    plane_start = D.plane_start;
+    pw_idx = D.pw_idx;
+    pw_pos = D.pw_pos;
+  }
   const int e0 = plane_start[zi], e1 = plane_start[zi + 1];
   for (int e = e0 + tid; e < e1; e += nt) {
     const int pos = pw_pos[e];
@@ -452,6 +460,16 @@ k_fwd_xy(LocalPlan p, int band0, const C2<double>* __restrict__ psi, long long l
   // gather the sphere (permuted x storage) and add the kinetic diagonal
   const C2<double>* ps = psi + (size_t)(band0 + b) * ldpsi;
   C2<double>* hp = hpsi + (size_t)(band0 + b) * ldh;
+  if (p.kdesc) {      // batch of k-points: this band's own basis and block
+    const int2 r = p.bref[band0 + b];
+    const KDesc& D = p.kdesc[r.x];
+    ps = D.psi + (size_t)r.y * D.ldpsi;
+    hp = D.hpsi + (size_t)r.y * D.ldh;
+    plane_start = D.plane_start;
+    pw_idx = D.pw_idx;
+    pw_pos = D.pw_pos;
+    ekpg = D.ekpg;
+  }
   const int e0 = plane_start[zi], e1 = plane_start[zi + 1];
   for (int e = e0 + tid; e < e1; e += nt) {
     const int pos = pw_pos[e];
@@ -501,7 +519,8 @@ cudaError_t launch_impl(const LocalPlan& p, int nbc, int band0, const C2<double>
     kb<<<dim3((unsigned)tiles, nbc), kThreadsCols, sm_co, st>>>(p, vr, twz, W);
   } else {
     // column tiles x band groups: enough CTAs for two per SM on small boxes
-    long long groups = std::max(1LL, std::min((long long)nbc, (2LL * nsm + tiles - 1) / tiles));
+    const long long per_sm = p.bgroups > 0 ? p.bgroups : 2;
+    long long groups = std::max(1LL, std::min((long long)nbc, (per_sm * nsm + tiles - 1) / tiles));
     const int per = (int)((nbc + groups - 1) / groups);
     groups = (nbc + per - 1) / per;
     auto* kbp = k_z_vloc_pipe<T, RZ1, RZ2, CB>;

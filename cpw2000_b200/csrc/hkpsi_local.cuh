@@ -27,7 +27,25 @@ struct FftDim {
   int n, r1, r2;
 };
 
+// One k-point of a batch: its wavefunction blocks, its plane lists (relative to the
+// batch's common kept planes and rows) and its kinetic diagonal.
+struct KDesc {
+  const C2<double>* psi;
+  C2<double>* hpsi;
+  long long ldpsi, ldh;
+  const int* plane_start;
+  const int* pw_idx;
+  const int* pw_pos;
+  const double* ekpg;     // null: no kinetic term
+};
+
 struct LocalPlan {
+  // batch mode (null for one k-point): global band b of a launch is band bref[b].y of
+  // k-point bref[b].x, described by kdesc[bref[b].x]; the per-call pointer arguments
+  // of kernels A and C are then ignored
+  const KDesc* kdesc;
+  const int2* bref;
+  int bgroups;            // kernel B band grouping: 0 = heuristic, else target CTAs per SM
   int n1, n2, n3;         // FFT box
   int kd1, kd2, kd3;      // sphere half-widths (largest |k_j| of the basis)
   int nx, ny, nz;         // 2*kd+1

@@ -612,8 +612,27 @@ int grid_for(long long work, int nsm) {
 
 }  // namespace
 
-int tc_prepare_projectors(cpw_b200_ctx* c) {
-  const int m = c->mtxd, na = c->nanl;
+// the sticky error flag of the tensor-core kernels: zeroed when allocated, read and cleared by
+// tc_check_error (a bounded wait that gave up in any launch since the last check reports)
+int tc_error_flag(TcScratch& t) {
+  if (t.err.p) return kOk;
+  if (int s = t.err.ensure(sizeof(int))) return s;
+  cudaError_t e = cudaMemset(t.err.p, 0, sizeof(int));
+  return e == cudaSuccess ? kOk : cuda_fail(e, "tc error flag");
+}
+
+int tc_read_error(TcScratch& t) {
+  if (!t.err.p) return kOk;
+  int h = 0;
+  cudaError_t e = cudaMemcpy(&h, t.err.p, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "tc error flag");
+  if (!h) return kOk;
+  cudaMemset(t.err.p, 0, sizeof(int));
+  return fail(kTimeout, "tensor-core GEMM: an mbarrier wait gave up");
+}
+
+int tc_prepare_operands(int m, int na, const void* anl, const void* anld, DevBuf& a1buf, DevBuf& a2buf,
+                        long long* nkb1_out, long long* nkb2_out, cudaStream_t st) {
   if (na == 0 || m == 0) return kOk;
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
@@ -622,28 +641,34 @@ int tc_prepare_projectors(cpw_b200_ctx* c) {
   const long long nkb2 = (2LL * na + tc::BK - 1) / tc::BK;
   const size_t fa1 = tc::tiled_floats(2 * na, nkb1), fa2 = tc::tiled_floats(m, nkb2);
   int s;
-  if ((s = c->tc_a1.ensure(sizeof(float) * 2 * fa1)) || (s = c->tc_a2.ensure(sizeof(float) * 2 * fa2))) return s;
-  float* a1 = (float*)c->tc_a1.p;
-  float* a2 = (float*)c->tc_a2.p;
-  tc::k_prep_a1<<<grid_for(2LL * na * nkb1 * 16, nsm), 256, 0, c->stream>>>(m, na, nkb1, (const C2<double>*)c->anl.p,
-                                                                              a1, a1 + fa1);
-  tc::k_prep_a2<<<grid_for((long long)m * nkb2 * 16, nsm), 256, 0, c->stream>>>(m, na, nkb2,
-                                                                                 (const C2<double>*)c->anld.p, a2,
-                                                                                 a2 + fa2);
-  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if ((s = a1buf.ensure(sizeof(float) * 2 * fa1)) || (s = a2buf.ensure(sizeof(float) * 2 * fa2))) return s;
+  float* a1 = (float*)a1buf.p;
+  float* a2 = (float*)a2buf.p;
+  tc::k_prep_a1<<<grid_for(2LL * na * nkb1 * 16, nsm), 256, 0, st>>>(m, na, nkb1, (const C2<double>*)anl, a1, a1 + fa1);
+  tc::k_prep_a2<<<grid_for((long long)m * nkb2 * 16, nsm), 256, 0, st>>>(m, na, nkb2, (const C2<double>*)anld, a2,
+                                                                          a2 + fa2);
+  cudaError_t e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return cuda_fail(e, "tensor-core projector preparation");
-  c->tc_k1p = nkb1;
-  c->tc_k2p = nkb2;
+  *nkb1_out = nkb1;
+  *nkb2_out = nkb2;
+  return kOk;
+}
+
+int tc_prepare_projectors(cpw_b200_ctx* c) {
+  if (c->nanl == 0 || c->mtxd == 0) return kOk;
+  int s = tc_prepare_operands(c->mtxd, c->nanl, c->anl.p, c->anld.p, c->tc_a1, c->tc_a2, &c->tc_k1p, &c->tc_k2p,
+                              c->stream);
+  if (s) return s;
   c->tc_ready = true;
   return kOk;
 }
 
-// hpsi += X D X^H psi in split TF32 on the tensor cores (hpsi already holds the local part)
-int tc_nl_apply(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh, cudaStream_t st,
-                cudaEvent_t t0, cudaEvent_t t1, cudaEvent_t t2) {
-  if (!c->tc_ready) return fail(kNotReady, "tensor-core projectors not prepared");
-  const int m = c->mtxd, na = c->nanl;
-  const long long nkb1 = c->tc_k1p, nkb2 = c->tc_k2p;
+// hpsi += X D X^H psi in split TF32 on the tensor cores (hpsi already holds the local part);
+// a1/a2 are the tiled operands of tc_prepare_operands for (m, na); scratch and the error
+// flag are the context's
+int tc_nl_apply_ops(TcScratch& t, int m, int na, long long nkb1, long long nkb2, const float* a1, const float* a2,
+                    int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh, cudaStream_t st,
+                    cudaEvent_t t0, cudaEvent_t t1, cudaEvent_t t2, int splits) {
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -652,20 +677,21 @@ int tc_nl_apply(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void*
 
   // GEMM 1: (2 nanl) x nb, K = 2 mtxd, split over K so that the work items fill the SMs about once
   const int mt1 = (2 * na + tc::BM - 1) / tc::BM, nt1 = (nb + tc::BN - 1) / tc::BN;
+  // splits: 0 = about one work item per SM, > 0 that many, -d a d-th of the default
   int nsplit = std::max(1, (int)std::min<long long>(nkb1, nsm / (mt1 * nt1)));
+  if (splits < 0) nsplit = std::max(1, nsplit / -splits);
+  if (splits > 0) nsplit = (int)std::min<long long>(nkb1, splits);
   if (const int ks = env_int("CPW_B200_TC_SPLITS", 0)) nsplit = (int)std::max(1LL, std::min<long long>(nkb1, ks));
   const int kbps = (int)((nkb1 + nsplit - 1) / nsplit);
   nsplit = (int)((nkb1 + kbps - 1) / kbps);
   const size_t fb1 = tc::tiled_floats(nb, nkb1), fb2 = tc::tiled_floats(2 * nb, nkb2);
   int s;
-  if ((s = c->tc_b1.ensure(sizeof(float) * 2 * fb1)) ||
-      (s = c->tc_part.ensure(sizeof(double) * (size_t)nsplit * nb * 2 * na)) ||
-      (s = c->tc_b2.ensure(sizeof(float) * 2 * fb2)) || (s = c->tc_err.ensure(sizeof(int))))
+  if ((s = t.b1.ensure(sizeof(float) * 2 * fb1)) ||
+      (s = t.part.ensure(sizeof(double) * (size_t)nsplit * nb * 2 * na)) ||
+      (s = t.b2.ensure(sizeof(float) * 2 * fb2)) || (s = tc_error_flag(t)))
     return s;
-  float* b1 = (float*)c->tc_b1.p;
-  float* b2 = (float*)c->tc_b2.p;
-  const float* a1 = (const float*)c->tc_a1.p;
-  const float* a2 = (const float*)c->tc_a2.p;
+  float* b1 = (float*)t.b1.p;
+  float* b2 = (float*)t.b2.p;
   const size_t fa1 = tc::tiled_floats(2 * na, nkb1), fa2 = tc::tiled_floats(m, nkb2);
 
   tc::GemmArgs g1{};
@@ -683,8 +709,8 @@ int tc_nl_apply(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void*
   g1.tiles_n = nt1;
   g1.n_fast = 0;
   g1.terms = terms;
-  g1.out = (double*)c->tc_part.p;
-  g1.err = (int*)c->tc_err.p;
+  g1.out = (double*)t.part.p;
+  g1.err = (int*)t.err.p;
 
   // GEMM 2: mtxd x (2 nb), K = 2 nanl, added into hpsi
   const int mt2 = (m + tc::BM - 1) / tc::BM, nt2 = (2 * nb + tc::BN - 1) / tc::BN;
@@ -705,10 +731,9 @@ int tc_nl_apply(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void*
   g2.terms = terms;
   g2.out = (double*)hpsi;
   g2.ldh = ldh;
-  g2.err = (int*)c->tc_err.p;
+  g2.err = (int*)t.err.p;
 
-  cudaError_t e = cudaMemsetAsync(c->tc_err.p, 0, sizeof(int), st);
-  if (e != cudaSuccess) return cuda_fail(e, "tc nl");
+  cudaError_t e;
   if ((e = cudaFuncSetAttribute(tc::k_gemm_tf32x3<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 tc::kSmemBytes)) != cudaSuccess ||
       (e = cudaFuncSetAttribute(tc::k_gemm_tf32x3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -722,13 +747,20 @@ int tc_nl_apply(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void*
   if ((2LL * na) % tc::BK) {
     if ((e = cudaMemsetAsync(b2, 0, sizeof(float) * 2 * fb2, st)) != cudaSuccess) return cuda_fail(e, "tc nl");
   }
-  tc::k_reduce_p<<<grid_for((long long)na * nb, nsm), 256, 0, st>>>(na, nb, nsplit, nkb2, (const double*)c->tc_part.p,
+  tc::k_reduce_p<<<grid_for((long long)na * nb, nsm), 256, 0, st>>>(na, nb, nsplit, nkb2, (const double*)t.part.p,
                                                                     b2, b2 + fb2);
   if (t1) cudaEventRecord(t1, st);
   tc::k_gemm_tf32x3<1><<<std::min(items2, nsm), tc::kThreads, tc::kSmemBytes, st>>>(g2);
   if (t2) cudaEventRecord(t2, st);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "tensor-core projector GEMMs");
   return kOk;
+}
+
+int tc_nl_apply(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh, cudaStream_t st,
+                cudaEvent_t t0, cudaEvent_t t1, cudaEvent_t t2) {
+  if (!c->tc_ready) return fail(kNotReady, "tensor-core projectors not prepared");
+  return tc_nl_apply_ops(c->tcs, c->mtxd, c->nanl, c->tc_k1p, c->tc_k2p, (const float*)c->tc_a1.p,
+                         (const float*)c->tc_a2.p, nb, psi, ldpsi, hpsi, ldh, st, t0, t1, t2);
 }
 
 // C (m x n) = A (m x kk) B (kk x n), complex128 column-major, in split TF32 on the tensor cores
@@ -745,7 +777,7 @@ int tc_zgemm_nn(cpw_b200_ctx* c, int m, int n, int kk, const void* a, long long 
   const size_t fa = tc::tiled_floats(m, nkb), fb = tc::tiled_floats(2LL * n, nkb);
   int s;
   if ((s = c->tc_ga.ensure(sizeof(float) * 2 * fa)) || (s = c->tc_gb.ensure(sizeof(float) * 2 * fb)) ||
-      (s = c->tc_err.ensure(sizeof(int))))
+      (s = tc_error_flag(c->tcs)))
     return s;
   float* ga = (float*)c->tc_ga.p;
   float* gb = (float*)c->tc_gb.p;
@@ -771,7 +803,7 @@ int tc_zgemm_nn(cpw_b200_ctx* c, int m, int n, int kk, const void* a, long long 
   g.terms = 3;
   g.out = (double*)cm;
   g.ldh = ldc;
-  g.err = (int*)c->tc_err.p;
+  g.err = (int*)c->tcs.err.p;
   if ((e = cudaFuncSetAttribute(tc::k_gemm_tf32x3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 tc::kSmemBytes)) != cudaSuccess)
     return cuda_fail(e, "tensor-core GEMM attribute");
@@ -780,12 +812,6 @@ int tc_zgemm_nn(cpw_b200_ctx* c, int m, int n, int kk, const void* a, long long 
   return kOk;
 }
 
-int tc_check_error(cpw_b200_ctx* c) {
-  if (!c->tc_err.p) return kOk;
-  int h = 0;
-  cudaError_t e = cudaMemcpy(&h, c->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost);
-  if (e != cudaSuccess) return cuda_fail(e, "tc error flag");
-  return h ? fail(kTimeout, "tensor-core GEMM: an mbarrier wait gave up") : kOk;
-}
+int tc_check_error(cpw_b200_ctx* c) { return tc_read_error(c->tcs); }
 
 }  // namespace cpwb

@@ -174,6 +174,43 @@ void ditsp_c16_(const int* ipr, int* ifail, const int* icmax, const int* iguess,
                 const double* hdiag, const int* mxddim, const int* mxdsml, const int* mxdbnd, const int* mxdgve,
                 const int* mxdscr, const int* mxdanl);
 
+/* ---- batched k-points ----
+ * No counterpart in the reference, which applies H one k-point at a time
+ * (Src/cpw_lib/cpw_scf.f90:488 -> h_kb_dia -> ditsp_c16 -> hk_psi_c16). A batch
+ * holds the bases of nk k-points of one crystal (one FFT box, the context's
+ * potential, one projector set per k-point) and applies
+ * hpsi_k = H_k psi_k (hk_psi_c16.f90:28-241 per k) to all of them in one call:
+ * one launch per local stage over the bands of every k-point (uneven plane-wave
+ * and band counts), then the projector products of each k-point. The first
+ * call with a given set of arrays and band counts times a small set of launch
+ * shapes (autotuning), runs the fastest and captures it as a CUDA graph; later
+ * calls with the same arrays and counts replay the graph. The precision is the
+ * context's at creation (FP64, MIXED or MIXED_TC); the potential is the
+ * context's (cpw_b200_set_potential), set before the first call.
+ *
+ * create: mtxd[k], isort[k] (1-based into kgv, reference layout), ekpg[k] are
+ *   host arrays per k-point; kgv(3, ng) and kmscr(7) are shared. The context
+ *   keeps k-point 0 as its own basis.
+ * set_projectors: host anlga(ld, nanl) complex128 column-major (first mtxd[ik]
+ *   rows used) and xnlkb(nanl) of k-point ik (proj_nl_kb_c16.f90 output).
+ * hk_psi_device: per k-point device blocks psi[k], hpsi[k] (complex128,
+ *   column-major, leading dimensions ldpsi[k], ldh[k] >= mtxd[k]) of nb[k]
+ *   bands; stream: cudaStream_t the call is ordered after and before.
+ * synchronize: waits for the batch's work; CPW_B200_TIMEOUT if a bounded wait
+ *   in a tensor-core kernel gave up.
+ * info: out[0..n) = {tuned, chunk bands, kernel B grouping, projection split
+ *   setting, tuned call time in us, candidates timed, graph replays, captures}. */
+typedef struct cpw_b200_kbatch cpw_b200_kbatch;
+int cpw_b200_kbatch_create(cpw_b200_ctx* ctx, int nk, const int* mtxd, const int* const* isort, const int* kgv,
+                           int ng, const double* const* ekpg, const int* kmscr, cpw_b200_kbatch** out);
+int cpw_b200_kbatch_destroy(cpw_b200_kbatch* b);
+int cpw_b200_kbatch_set_projectors(cpw_b200_kbatch* b, int ik, int nanl, const void* anlga, long long ld,
+                                   const double* xnlkb);
+int cpw_b200_kbatch_hk_psi_device(cpw_b200_kbatch* b, const int* nb, void* const* psi, const long long* ldpsi,
+                                  void* const* hpsi, const long long* ldh, void* stream);
+int cpw_b200_kbatch_synchronize(cpw_b200_kbatch* b);
+int cpw_b200_kbatch_info(cpw_b200_kbatch* b, long long* out, int n);
+
 /* ---- allocation-free local H|psi> ----
  * No counterpart in the reference. For callers that cannot call cudaMalloc
  * (a caller-owned memory pool or fixed device-memory budget, a host code that
