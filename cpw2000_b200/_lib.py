@@ -51,6 +51,7 @@ SIGNATURES = {
     "cpw_b200_density_device": (I, [P, I, P, LL, DP, P, P]),
     "cpw_b200_structure_grad_device": (I, [P, P, I, IP, DP, I, P, DP, P]),
     "cpw_b200_nl_grad_device": (I, [P, I, P, LL, DP, IP, I, DP, P]),
+    "cpw_b200_stress_inputs_device": (I, [P, I, P, LL, DP, P, P, P]),
     "cpw_b200_ditsp_device": (I, [P, I, IP, I, I, C.c_double, IP, I, P, LL, P, DP, DP, I, DP, I,
                                   C.POINTER(C.c_longlong), P, DP, I]),
     "cpw_b200_ditsp_c16": (I, [IP, IP, IP, IP, DP, IP, IP, IP, IP, DP, DP, DP, DP, IP, DP, IP, IP, IP, DP, DP, IP,

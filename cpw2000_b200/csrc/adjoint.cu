@@ -200,7 +200,79 @@ __global__ void k_nl_contract(int nanl, int nb, const Z* __restrict__ P, const Z
   }
 }
 
+// w(i) = sum_n f_n |c_n(i)|^2 (the kinetic stress weight of plane wave i)
+__global__ void k_band_weights(int m, int nb, const Z* __restrict__ psi, long long ld, const double* __restrict__ f,
+                               double* __restrict__ w) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int n = 0; n < nb; ++n) {
+      const Z c = psi[(size_t)n * ld + i];
+      s += f[n] * (c.x * c.x + c.y * c.y);
+    }
+    w[i] = s;
+  }
+}
+
+// M(n, a) = f_n conj(P(a, n)) xnlkb(a), M (nb x nanl) column-major
+__global__ void k_stress_m(int nanl, int nb, const Z* __restrict__ P, const double* __restrict__ f,
+                           const double* __restrict__ xnl, Z* __restrict__ M) {
+  const long long n = (long long)nanl * nb;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int a = (int)(t / nb), b = (int)(t - (long long)a * nb);
+    const Z p = P[(size_t)b * nanl + a];
+    const double s = f[b] * xnl[a];
+    M[(size_t)a * nb + b] = make_cuDoubleComplex(s * p.x, -s * p.y);
+  }
+}
+
 }  // namespace
+
+// The two blocks the strain derivative of E = sum_n f_n <psi_n|H|psi_n> needs besides the
+// density: w(i) = sum_n f_n |c_n(i)|^2 (kinetic) and Y = psi diag(f) P^H diag(xnlkb)
+// (mtxd x nanl, KB term: dE = 2 Re sum conj(dX) Y for a change dX of the projectors).
+int stress_inputs_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, const double* occ, double* w,
+                         void* y, cudaStream_t st) {
+  if (!c->have_basis) return fail(kNotReady, "stress inputs: basis must be set");
+  const int na = c->nanl, m = c->mtxd;
+  if (nb < 0 || ldpsi < m) return fail(kBadArg, "stress inputs: invalid block");
+  if (m == 0) return kOk;
+  int s;
+  DevBuf P, M, docc, dxnl;
+  if ((s = docc.ensure(sizeof(double) * std::max(nb, 1)))) return s;
+  cudaError_t e;
+  if (nb > 0 && (e = cudaMemcpyAsync(docc.p, occ, sizeof(double) * nb, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return cuda_fail(e, "stress inputs occ");
+  if (nb == 0) {
+    if ((e = cudaMemsetAsync(w, 0, sizeof(double) * m, st)) != cudaSuccess) return cuda_fail(e, "stress inputs");
+  } else {
+    k_band_weights<<<std::min(1184, (m + 255) / 256), 256, 0, st>>>(m, nb, (const Z*)psi, ldpsi,
+                                                                   (const double*)docc.p, w);
+  }
+  if (na > 0) {
+    if (nb == 0) {
+      if ((e = cudaMemsetAsync(y, 0, sizeof(Z) * (size_t)m * na, st)) != cudaSuccess) return cuda_fail(e, "stress");
+    } else {
+      if ((s = P.ensure(sizeof(Z) * (size_t)na * nb)) || (s = M.ensure(sizeof(Z) * (size_t)na * nb)) ||
+          (s = dxnl.ensure(sizeof(double) * na)))
+        return s;
+      if ((e = cudaMemcpyAsync(dxnl.p, c->xnl_h.data(), sizeof(double) * na, cudaMemcpyHostToDevice, st)) !=
+          cudaSuccess)
+        return cuda_fail(e, "stress inputs xnlkb");
+      cublasSetStream(c->blas, st);
+      const Z one = make_cuDoubleComplex(1, 0), zero = make_cuDoubleComplex(0, 0);
+      cublasStatus_t bs = cublasZgemm(c->blas, CUBLAS_OP_C, CUBLAS_OP_N, na, nb, m, &one, (const Z*)c->anl.p, m,
+                                      (const Z*)psi, (int)ldpsi, &zero, (Z*)P.p, na);
+      if (bs != CUBLAS_STATUS_SUCCESS) return fail(kCublas, "stress inputs zgemm P");
+      k_stress_m<<<std::max(1, std::min(1184, (na * nb + 255) / 256)), 256, 0, st>>>(
+          na, nb, (const Z*)P.p, (const double*)docc.p, (const double*)dxnl.p, (Z*)M.p);
+      bs = cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, m, na, nb, &one, (const Z*)psi, (int)ldpsi, (const Z*)M.p,
+                       nb, &zero, (Z*)y, m);
+      if (bs != CUBLAS_STATUS_SUCCESS) return fail(kCublas, "stress inputs zgemm Y");
+    }
+  }
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "stress inputs");
+  return kOk;
+}
 
 int density_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, const double* occ, void* rho,
                    cudaStream_t st) {

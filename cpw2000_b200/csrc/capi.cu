@@ -405,6 +405,13 @@ int cpw_b200_nl_grad_device(cpw_b200_ctx* c, int neig, const void* psi, long lon
   return nl_grad_device(c, neig, psi, ldpsi, occ, proj_atom, natom, dedtau, stream ? (cudaStream_t)stream : c->stream);
 }
 
+int cpw_b200_stress_inputs_device(cpw_b200_ctx* c, int neig, const void* psi, long long ldpsi, const double* occ,
+                                  double* w, void* y, void* stream) {
+  if (int s = check_ctx(c)) return s;
+  cudaSetDevice(c->device);
+  return stress_inputs_device(c, neig, psi, ldpsi, occ, w, y, stream ? (cudaStream_t)stream : c->stream);
+}
+
 int cpw_b200_hk_psi_nl_c16(const int* mtxd, const int* neig, const double* psi, double* hpsi, const double* anlga,
                            const double* xnlkb, const int* nanl, const int* ladd, const int* mxddim,
                            const int* mxdbnd, const int* mxdanl) {

@@ -83,6 +83,8 @@ int density_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, co
                    cudaStream_t st);
 int structure_grad_device(cpw_b200_ctx* c, const void* g, int natom, const int* atom_type, const double* tau,
                           int ntype, const void* vgt, double* dedtau, cudaStream_t st);
+int stress_inputs_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, const double* occ, double* w,
+                         void* y, cudaStream_t st);
 int nl_grad_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, const double* occ,
                    const int* proj_atom, int natom, double* dedtau, cudaStream_t st);
 }  // namespace cpwb

@@ -119,6 +119,13 @@ int cpw_b200_structure_grad_device(cpw_b200_ctx* ctx, const void* g, int natom, 
                                    const double* tau, int ntype, const void* vgt, double* dedtau, void* stream);
 int cpw_b200_nl_grad_device(cpw_b200_ctx* ctx, int neig, const void* psi, long long ldpsi, const double* occ,
                             const int* proj_atom, int natom, double* dedtau, void* stream);
+/* stress_inputs: the blocks the strain derivative (stress) of sum_n occ_n <psi_n|H|psi_n> needs
+ *   besides the density (Src/ALFA/for_str_kinetic_stress.f90, for_str_nl_kb.f90:364-376):
+ *   w (device, mtxd doubles) = sum_n occ_n |psi(i,n)|^2 and y (device, mtxd x nanl
+ *   complex128, ld mtxd) = psi diag(occ) P^H diag(xnlkb) with P = X^H psi for the context's
+ *   projectors X; a change dX of the projectors changes the KB energy by 2 Re sum conj(dX) y. */
+int cpw_b200_stress_inputs_device(cpw_b200_ctx* ctx, int neig, const void* psi, long long ldpsi, const double* occ,
+                                  double* w, void* y, void* stream);
 
 /* ---- drop-ins with the reference argument lists ---- */
 
