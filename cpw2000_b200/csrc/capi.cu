@@ -15,6 +15,7 @@ const char* last_error();
 }
 
 using namespace cpwb;
+using C2d = C2<double>;
 
 namespace {
 
@@ -77,6 +78,73 @@ int d2h_cols(double* dst, long long ldd, const void* src, long long lds, long lo
   return e == cudaSuccess ? kOk : cuda_fail(e, "cudaMemcpy2D D2H");
 }
 
+
+// H|psi> of host blocks (ld mxddim) through the device buffers h_in / h_out, pipelined over
+// band chunks: every chunk's copy to the device is issued first on its own stream (the caller
+// checks its other inputs on the host meanwhile), chunk k is computed once its copy landed, and
+// its copy back runs on a third stream while chunk k+1 is computed (with page-locked host
+// arrays the three overlap; pageable arrays degrade to staged copies). Results are the same
+// as one pass: every band's H|psi> depends on that band only.
+struct DropinPipe {
+  int m = 0, nb = 0, chunk = 0, nchunk = 0;
+  long long ldh = 0;
+};
+
+int dropin_stage_in(cpw_b200_ctx* c, int m, int nb, const double* psi, long long ldh_host, DropinPipe* pp) {
+  constexpr int kChunks = 8, kMinChunk = 16;
+  DropinPipe& p = *pp;
+  p.m = m;
+  p.nb = nb;
+  p.ldh = ldh_host;
+  p.chunk = std::max(kMinChunk, (nb + kChunks - 1) / kChunks);
+  p.nchunk = (nb + p.chunk - 1) / p.chunk;
+  cudaError_t e;
+  if (!c->s_in && (e = cudaStreamCreateWithFlags(&c->s_in, cudaStreamNonBlocking)) != cudaSuccess)
+    return cuda_fail(e, "hk_psi_c16 stream");
+  if (!c->s_out && (e = cudaStreamCreateWithFlags(&c->s_out, cudaStreamNonBlocking)) != cudaSuccess)
+    return cuda_fail(e, "hk_psi_c16 stream");
+  while ((int)c->ev_pipe.size() < 2 * p.nchunk + 1) {
+    cudaEvent_t ev;
+    if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return cuda_fail(e, "event");
+    c->ev_pipe.push_back(ev);
+  }
+  // the copy-in stream starts after any earlier work on the compute stream (h_in reuse)
+  cudaEvent_t start = c->ev_pipe[2 * p.nchunk];
+  if ((e = cudaEventRecord(start, c->stream)) != cudaSuccess || (e = cudaStreamWaitEvent(c->s_in, start, 0)) != cudaSuccess)
+    return cuda_fail(e, "hk_psi_c16 pipeline");
+  C2d* din = (C2d*)c->h_in.p;
+  for (int k = 0; k < p.nchunk; ++k) {
+    const int b0 = k * p.chunk, nbc = std::min(p.chunk, nb - b0);
+    if (int s = h2d_cols(din + (size_t)b0 * m, m, psi + 2 * (size_t)b0 * ldh_host, ldh_host, m, nbc, c->s_in)) return s;
+    if ((e = cudaEventRecord(c->ev_pipe[2 * k], c->s_in)) != cudaSuccess) return cuda_fail(e, "hk_psi_c16 pipeline");
+  }
+  return kOk;
+}
+
+int dropin_compute_out(cpw_b200_ctx* c, const DropinPipe& p, double* hpsi) {
+  cudaError_t e;
+  const int m = p.m;
+  C2d* din = (C2d*)c->h_in.p;
+  C2d* dout = (C2d*)c->h_out.p;
+  for (int k = 0; k < p.nchunk; ++k) {
+    const int b0 = k * p.chunk, nbc = std::min(p.chunk, p.nb - b0);
+    cudaEvent_t in_done = c->ev_pipe[2 * k], out_ready = c->ev_pipe[2 * k + 1];
+    if ((e = cudaStreamWaitEvent(c->stream, in_done, 0)) != cudaSuccess) return cuda_fail(e, "hk_psi_c16 pipeline");
+    if (int s = ctx_hkpsi_device(c, nbc, din + (size_t)b0 * m, m, dout + (size_t)b0 * m, m, c->stream, true, true))
+      return s;
+    if ((e = cudaEventRecord(out_ready, c->stream)) != cudaSuccess || (e = cudaStreamWaitEvent(c->s_out, out_ready, 0)) != cudaSuccess)
+      return cuda_fail(e, "hk_psi_c16 pipeline");
+    if (int s = d2h_cols(hpsi + 2 * (size_t)b0 * p.ldh, p.ldh, dout + (size_t)b0 * m, m, m, nbc, c->s_out)) return s;
+  }
+  if ((e = cudaStreamSynchronize(c->s_out)) != cudaSuccess) return cuda_fail(e, "hk_psi_c16");
+  if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return cuda_fail(e, "hk_psi_c16");
+  return kOk;
+}
+
+// wait for copies already issued (an error path must not leave them reading freed buffers)
+void dropin_abandon(cpw_b200_ctx* c) {
+  if (c->s_in) cudaStreamSynchronize(c->s_in);
+}
 
 // Bring the default context in line with the arguments of a drop-in call: the
 // k-point arrays and vscr are compared with the previous call's shadows and
@@ -159,6 +227,11 @@ int cpw_b200_destroy(cpw_b200_ctx* c) {
   if (!c) return kOk;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  if (c->s_in) cudaStreamSynchronize(c->s_in);
+  if (c->s_out) cudaStreamSynchronize(c->s_out);
+  for (cudaEvent_t e : c->ev_pipe) cudaEventDestroy(e);
+  if (c->s_in) cudaStreamDestroy(c->s_in);
+  if (c->s_out) cudaStreamDestroy(c->s_out);
   if (c->blas) cublasDestroy(c->blas);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -293,18 +366,25 @@ int cpw_b200_hk_psi_c16(const int* mtxd, const int* neig, const double* psi, dou
   cudaSetDevice(c->device);
   const int m = *mtxd, nb = *neig;
   int s;
+  // start the wavefunction copies (device buffers sized by mtxd and neig alone), then bring
+  // the context in line with the other inputs on the host while they travel
+  DropinPipe pipe;
+  const bool go = m > 0 && nb > 0;
+  if (go) {
+    const size_t bytes = (size_t)m * nb * 16;
+    if ((s = c->h_in.ensure(bytes)) || (s = c->h_out.ensure(bytes)) ||
+        (s = dropin_stage_in(c, m, nb, psi, *mxddim, &pipe))) {
+      dropin_abandon(c);
+      return s;
+    }
+  }
   if ((s = sync_dropin_inputs(c, m, *ng, kgv, ekpg, isort, vscr, kmscr, anlga, xnlkb, *nanl, *mxddim, *mxdscr,
-                              lnewanl)))
+                              lnewanl))) {
+    dropin_abandon(c);
     return s;
-  if (m == 0 || nb == 0) return kOk;
-  const size_t bytes = (size_t)m * nb * 16;
-  if ((s = c->h_in.ensure(bytes))) return s;
-  if ((s = c->h_out.ensure(bytes))) return s;
-  if ((s = h2d_cols(c->h_in.p, m, psi, *mxddim, m, nb, c->stream))) return s;
-  if ((s = ctx_hkpsi_device(c, nb, c->h_in.p, m, c->h_out.p, m, c->stream, true, true))) return s;
-  if ((s = d2h_cols(hpsi, *mxddim, c->h_out.p, m, m, nb, c->stream))) return s;
-  cudaError_t e = cudaStreamSynchronize(c->stream);
-  return e == cudaSuccess ? kOk : cuda_fail(e, "hk_psi_c16");
+  }
+  if (!go) return kOk;
+  return dropin_compute_out(c, pipe, hpsi);
 }
 
 void hk_psi_c16_(const int* mtxd, const int* neig, const double* psi, double* hpsi, int* lnewanl, const int* ng,

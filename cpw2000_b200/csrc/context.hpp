@@ -92,6 +92,9 @@ int nl_grad_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, co
 struct cpw_b200_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // drop-in host path: copy streams and per-chunk events of the pipelined transfer
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  std::vector<cudaEvent_t> ev_pipe;
   cublasHandle_t blas = nullptr;
   int precision = 0;            // 0: FP64; 1: FP32 local + FP64 projector GEMMs; 2: 1 with split-TF32 tensor-core projectors
   size_t slab_budget = 512ull << 20;

@@ -232,3 +232,26 @@ def test_mixed_tc_edge_shapes(cuda, wname, nb):
         if prec == H.MIXED_TC:
             assert relerr(full, oracle_hpsi(d, psi, nb)) < TOL32
     assert relerr(nl[H.MIXED_TC], nl[H.FP64]) < 1e-7
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_dropin_pipelined_band_chunks(cuda, pinned):
+    """Drop-in hk_psi_c16 with 70 bands (five 16-band chunks, the last partial): the pipelined
+    host transfers give the oracle's result; with page-locked host arrays the copies overlap."""
+    import torch
+    w = configs.si2_fcc()
+    d = configs.kpoint_inputs(w, 2)
+    m, nb = d["mtxd"], 70
+    mxddim, mxdbnd = m + 3, nb + 1
+    psi = configs.random_psi(m, mxdbnd, 71, ld=mxddim)
+    hpsi = np.full((mxddim, mxdbnd), 5.0 - 5.0j, dtype=np.complex128, order="F")
+    if pinned:
+        tp = torch.from_numpy(psi.ravel(order="F").view(np.float64)).pin_memory()
+        th = torch.from_numpy(hpsi.ravel(order="F").view(np.float64)).pin_memory()
+        psi = tp.numpy().view(np.complex128).reshape((mxddim, mxdbnd), order="F")
+        hpsi = th.numpy().view(np.complex128).reshape((mxddim, mxdbnd), order="F")
+    anl = np.asfortranarray(np.vstack([d["anlga"], np.zeros((3, d["nanl"]), np.complex128)]))
+    H.hk_psi_c16(m, nb, psi, hpsi, True, d["ng"], np.asfortranarray(d["kgv"]), d["ekpg"], d["isort"], d["vscr"],
+                 d["kmscr"], anl, d["xnlkb"], d["nanl"], mxddim, mxdbnd, d["nanl"], d["ng"], d["vscr"].size)
+    assert relerr(hpsi[:m, :nb], oracle_hpsi(d, psi[:m], nb)) < TOL64
+    assert np.all(hpsi[m:, :] == 5.0 - 5.0j) and np.all(hpsi[:, nb:] == 5.0 - 5.0j)
