@@ -1,5 +1,5 @@
 /*
- * C + OpenMP restatement of cpw2000's hk_psi_c16 -- TEST / BASELINE INFRASTRUCTURE ONLY.
+ * C + OpenMP restatement of cpw2000's hk_psi_c16 -- TEST AND CPU-TIMING INFRASTRUCTURE ONLY.
  *
  * Follows the loop structure of Src/hk_psi/reference/hk_psi_c16.f90:176-231:
  * per band, zero the box, scatter psi into ipoint, backward pruned 3D FFT
