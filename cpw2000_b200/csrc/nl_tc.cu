@@ -20,15 +20,15 @@
 // stage is then four contiguous bulk copies (cp.async.bulk, no tensor map) of
 // rows x 128 bytes, whole DRAM pages instead of 128-byte pieces of 128 rows.
 //
-// Kernel (persistent: grid <= SM count, work items = output tile x K range, 10 warps):
+// Kernel (persistent: grid <= SM count, work items = output tile x K range, 18 warps):
 //   warp 0      producer: bulk copies of A hi/lo and B hi/lo into a 3-stage ring
 //               (full/empty mbarriers);
 //   warp 1      allocates 512 TMEM columns; one lane issues tcgen05.mma kind::tf32
 //               (M 128, N <= 128, K 8): hi.hi into one of three rotating main
 //               accumulators, restarted every `chain` K blocks; hi.lo and lo.hi into
 //               a correction accumulator that spans the whole work item;
-//   warps 2-9   drain: they read each finished main accumulator with tcgen05.ld and
-//               add it into FP64 sums in registers (one row and 64 columns per
+//   warps 2-17  drain: they read each finished main accumulator with tcgen05.ld and
+//               add it into FP64 sums in registers (one row and 32 columns per
 //               thread), release it, add the correction accumulator at the end of
 //               the work item, and store the tile.
 // The FP32 accumulation of the tensor cores shrinks a sum by a fixed fraction per
@@ -53,11 +53,13 @@ constexpr int kStages = 3;
 constexpr int kTileFloats = BM * BK;               // 4096 floats = 16 KB
 constexpr int kTileBytes = kTileFloats * 4;
 constexpr int kStageBytes = 4 * kTileBytes;        // A hi, A lo, B hi, B lo
-constexpr int kDrainWarps = 8;
+constexpr int kDrainWarps = 16;                   // 4 lane quarters x 4 column slices
+constexpr int kDrainCols = BN / (kDrainWarps / 4); // accumulator columns per drain thread
 constexpr int kThreads = 32 * (2 + kDrainWarps);
 constexpr int kBarBytes = 256;
 constexpr int kPrefetch = 8;                       // K blocks fetched into L2 ahead of the shared-memory copies
-constexpr int kEpiBytes = 2048;                    // per drain warp: 4 complex columns x 32 rows of FP64 staging
+constexpr int kEpiBytes = 1024;                    // per drain warp: 2 complex columns x 32 rows of FP64 staging
+constexpr int kEpiCplx = kEpiBytes / (32 * 16);
 constexpr int kSmemBytes = kStages * kStageBytes + 1024 + kBarBytes + kDrainWarps * kEpiBytes;
 constexpr unsigned long long kWaitNs = 2000000000ull;   // 2 s per mbarrier wait at most
 constexpr int kMainBufs = 3;                       // rotating hi.hi accumulators
@@ -368,15 +370,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
       if (!mbar_wait(smem_u32(done), 0u, nullptr)) atomicExch(g.err, 1);
     }
   } else {
-    const int quarter = warp & 3, half = (warp - 2) >> 2;
+    const int quarter = warp & 3, slice = (warp - 2) >> 2;
     const uint32_t lane_base = tmem + ((uint32_t)(32 * quarter) << 16);
     long long gq = 0;
     for (int it = blockIdx.x; it < nitems && !failed; it += gridDim.x) {
       const Item w = item_of(g, it);
       const int nchunk = (w.nblk + chain - 1) / chain;
-      double acc[64];
+      double acc[kDrainCols];
 #pragma unroll
-      for (int j = 0; j < 64; ++j) acc[j] = 0.0;
+      for (int j = 0; j < kDrainCols; ++j) acc[j] = 0.0;
       bool ok = true;
       for (int q = 0; q < nchunk; ++q, ++gq) {
         const int b = (int)(gq % kMainBufs);
@@ -392,8 +394,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
         for (int pass = 0; pass < (last ? 2 : 1); ++pass) {
           const uint32_t col0 = pass == 0 ? (uint32_t)((b + 1) * BN) : 0u;
 #pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const int col = 64 * half + 8 * j;
+          for (int j = 0; j < kDrainCols / 8; ++j) {
+            const int col = kDrainCols * slice + 8 * j;
             if (col < w.n_mma) {        // n_mma is a multiple of 16: whole 8-column pieces
               uint32_t r[8];
               tmem_ld8(lane_base + col0 + (uint32_t)col, r);
@@ -412,8 +414,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
       const int m = w.m0 + 32 * quarter + lane;
       if (nchunk > 0 && w.m0 + 32 * quarter < g.M) {      // warp-uniform: the warp has valid rows
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int col = 64 * half + 16 * j;
+        for (int j = 0; j < kDrainCols / 16; ++j) {
+          const int col = kDrainCols * slice + 16 * j;
           if (col < w.n_mma) {
             if (MODE == 0) {
 #pragma unroll
@@ -422,23 +424,24 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
                 if (n < g.N && m < g.M) g.out[((size_t)w.split * g.N + n) * g.M + m] = CPWB_ACC(16 * j + t);
               }
             } else {
-              // four complex columns at a time through this warp's staging slot: [column][32 rows] of
-              // (re, im), then one bulk FP64 add of 32 rows (512 contiguous bytes of hpsi) per column
+              // kEpiCplx complex columns at a time through this warp's staging slot: [column][32 rows]
+              // of (re, im), then one bulk FP64 add of 32 rows (512 contiguous bytes of hpsi) per column
               double2* slot = reinterpret_cast<double2*>(epi + (warp - 2) * kEpiBytes);
               const int rows = min(32, g.M - (w.m0 + 32 * quarter));
 #pragma unroll
-              for (int hh = 0; hh < 2; ++hh) {
-                const int c0 = w.n0 + col + 8 * hh;           // first real output column of the four
+              for (int hh = 0; hh < 8 / kEpiCplx; ++hh) {
+                const int c0 = w.n0 + col + 2 * kEpiCplx * hh;   // first real output column of the round
                 // the previous bulk adds must have finished reading the slot
                 asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
                 __syncwarp();
 #pragma unroll
-                for (int t = 0; t < 4; ++t)
-                  slot[t * 32 + lane] = make_double2(CPWB_ACC(16 * j + 8 * hh + 2 * t), CPWB_ACC(16 * j + 8 * hh + 2 * t + 1));
+                for (int t = 0; t < kEpiCplx; ++t)
+                  slot[t * 32 + lane] = make_double2(CPWB_ACC(16 * j + 2 * kEpiCplx * hh + 2 * t),
+                                                     CPWB_ACC(16 * j + 2 * kEpiCplx * hh + 2 * t + 1));
                 asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
                 __syncwarp();
                 if (lane == 0) {
-                  for (int t = 0; t < 4; ++t)
+                  for (int t = 0; t < kEpiCplx; ++t)
                     if (c0 + 2 * t + 1 < g.N)
                       bulk_add_f64(reinterpret_cast<double2*>(g.out) + (size_t)((c0 >> 1) + t) * g.ldh + (m - lane),
                                    smem_u32(slot + t * 32), (uint32_t)rows * 16u);
