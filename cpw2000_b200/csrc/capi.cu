@@ -91,7 +91,9 @@ struct DropinPipe {
 };
 
 int dropin_stage_in(cpw_b200_ctx* c, int m, int nb, const double* psi, long long ldh_host, DropinPipe* pp) {
-  constexpr int kChunks = 8, kMinChunk = 16;
+  int kChunks = 4;
+  constexpr int kMinChunk = 16;
+  if (const char* v = getenv("CPW_B200_DROPIN_CHUNKS")) kChunks = std::max(1, atoi(v));
   DropinPipe& p = *pp;
   p.m = m;
   p.nb = nb;
@@ -121,7 +123,14 @@ int dropin_stage_in(cpw_b200_ctx* c, int m, int nb, const double* psi, long long
   return kOk;
 }
 
-int dropin_compute_out(cpw_b200_ctx* c, const DropinPipe& p, double* hpsi) {
+int dropin_wait(cpw_b200_ctx* c) {
+  cudaError_t e;
+  if ((e = cudaStreamSynchronize(c->s_out)) != cudaSuccess) return cuda_fail(e, "hk_psi_c16");
+  if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return cuda_fail(e, "hk_psi_c16");
+  return kOk;
+}
+
+int dropin_compute_out(cpw_b200_ctx* c, const DropinPipe& p, double* hpsi, bool wait = true) {
   cudaError_t e;
   const int m = p.m;
   C2d* din = (C2d*)c->h_in.p;
@@ -136,9 +145,7 @@ int dropin_compute_out(cpw_b200_ctx* c, const DropinPipe& p, double* hpsi) {
       return cuda_fail(e, "hk_psi_c16 pipeline");
     if (int s = d2h_cols(hpsi + 2 * (size_t)b0 * p.ldh, p.ldh, dout + (size_t)b0 * m, m, m, nbc, c->s_out)) return s;
   }
-  if ((e = cudaStreamSynchronize(c->s_out)) != cudaSuccess) return cuda_fail(e, "hk_psi_c16");
-  if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return cuda_fail(e, "hk_psi_c16");
-  return kOk;
+  return wait ? dropin_wait(c) : kOk;
 }
 
 // wait for copies already issued (an error path must not leave them reading freed buffers)
@@ -146,13 +153,13 @@ void dropin_abandon(cpw_b200_ctx* c) {
   if (c->s_in) cudaStreamSynchronize(c->s_in);
 }
 
-// Bring the default context in line with the arguments of a drop-in call: the
-// k-point arrays and vscr are compared with the previous call's shadows and
-// re-uploaded only when they changed; the projectors when lnewanl is set, the
-// basis changed or nanl changed (then lnewanl is cleared).
-int sync_dropin_inputs(cpw_b200_ctx* c, int m, int ng, const int* kgv, const double* ekpg, const int* isort,
-                       const double* vscr, const int* kmscr, const double* anlga, const double* xnlkb, int nanl,
-                       int mxddim, int mxdscr, int* lnewanl) {
+// Bring the default context in line with the k-point arguments of a drop-in call: the
+// k-point arrays are compared with the previous call's shadows and re-uploaded only when
+// they changed; the projectors when lnewanl is set, the basis changed or nanl changed (then
+// lnewanl is cleared). The potential is the caller's next step (sync_dropin_potential).
+int sync_dropin_kpoint(cpw_b200_ctx* c, int m, int ng, const int* kgv, const double* ekpg, const int* isort,
+                       const int* kmscr, const double* anlga, const double* xnlkb, int nanl, int mxddim,
+                       int* lnewanl) {
   std::vector<int> kg((size_t)3 * m);
   for (int i = 0; i < m; ++i) {
     const int it = isort[i];
@@ -175,15 +182,21 @@ int sync_dropin_inputs(cpw_b200_ctx* c, int m, int ng, const int* kgv, const dou
     c->sh_ekpg.assign(ekpg, ekpg + m);
     c->sh_vscr.clear();
   }
-  const size_t nv = (size_t)kmscr[6] * kmscr[4] * kmscr[5];
-  if (!c->have_pot || !same(c->sh_vscr, vscr, nv)) {
-    if ((s = ctx_set_potential(c, vscr, mxdscr))) return s;
-    c->sh_vscr.assign(vscr, vscr + nv);
-  }
   if (kchanged || *lnewanl != 0 || c->nanl != nanl) {
     if ((s = ctx_set_projectors(c, nanl, anlga, mxddim, xnlkb, false))) return s;
     *lnewanl = 0;
   }
+  return kOk;
+}
+
+// vscr against the shadow of the potential on the device; uploads it when it differs
+int sync_dropin_potential(cpw_b200_ctx* c, const double* vscr, const int* kmscr, int mxdscr, bool* uploaded) {
+  const size_t nv = (size_t)kmscr[6] * kmscr[4] * kmscr[5];
+  *uploaded = false;
+  if (c->have_pot && same(c->sh_vscr, vscr, nv)) return kOk;
+  if (int s = ctx_set_potential(c, vscr, mxdscr)) return s;
+  c->sh_vscr.assign(vscr, vscr + nv);
+  *uploaded = true;
   return kOk;
 }
 
@@ -367,7 +380,7 @@ int cpw_b200_hk_psi_c16(const int* mtxd, const int* neig, const double* psi, dou
   const int m = *mtxd, nb = *neig;
   int s;
   // start the wavefunction copies (device buffers sized by mtxd and neig alone), then bring
-  // the context in line with the other inputs on the host while they travel
+  // the context in line with the k-point arguments on the host while they travel
   DropinPipe pipe;
   const bool go = m > 0 && nb > 0;
   if (go) {
@@ -378,12 +391,29 @@ int cpw_b200_hk_psi_c16(const int* mtxd, const int* neig, const double* psi, dou
       return s;
     }
   }
-  if ((s = sync_dropin_inputs(c, m, *ng, kgv, ekpg, isort, vscr, kmscr, anlga, xnlkb, *nanl, *mxddim, *mxdscr,
-                              lnewanl))) {
+  if ((s = sync_dropin_kpoint(c, m, *ng, kgv, ekpg, isort, kmscr, anlga, xnlkb, *nanl, *mxddim, lnewanl))) {
     dropin_abandon(c);
     return s;
   }
-  if (!go) return kOk;
+  bool uploaded = false;
+  if (!go || !c->have_pot) {
+    if ((s = sync_dropin_potential(c, vscr, kmscr, *mxdscr, &uploaded))) {
+      dropin_abandon(c);
+      return s;
+    }
+    return go ? dropin_compute_out(c, pipe, hpsi) : kOk;
+  }
+  // the potential on the device is the previous call's: compute with it while vscr is
+  // compared on the host (it changes only between SCF iterations); if it changed, upload
+  // it and compute again from the wavefunctions already on the device
+  if ((s = dropin_compute_out(c, pipe, hpsi, false))) {
+    dropin_wait(c);
+    return s;
+  }
+  const size_t nv = (size_t)kmscr[6] * kmscr[4] * kmscr[5];
+  if (same(c->sh_vscr, vscr, nv)) return dropin_wait(c);
+  if ((s = dropin_wait(c))) return s;
+  if ((s = sync_dropin_potential(c, vscr, kmscr, *mxdscr, &uploaded))) return s;
   return dropin_compute_out(c, pipe, hpsi);
 }
 
@@ -431,8 +461,9 @@ int cpw_b200_ditsp_c16(const int* ipr, int* ifail, const int* icmax, const int* 
   cudaSetDevice(c->device);
   const int m = *mtxd, nb = *mxdbnd;
   int s;
-  if ((s = sync_dropin_inputs(c, m, *ng, kgv, ekpg, isort, vscr, kmscr, anlga, xnlkb, *nanl, *mxddim, *mxdscr,
-                              lnewanl)))
+  bool uploaded = false;
+  if ((s = sync_dropin_kpoint(c, m, *ng, kgv, ekpg, isort, kmscr, anlga, xnlkb, *nanl, *mxddim, lnewanl)) ||
+      (s = sync_dropin_potential(c, vscr, kmscr, *mxdscr, &uploaded)))
     return s;
   const size_t bytes = (size_t)m * nb * 16;
   if ((s = c->h_in.ensure(bytes))) return s;
