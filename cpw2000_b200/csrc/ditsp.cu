@@ -265,6 +265,23 @@ __global__ void __launch_bounds__(256) k_mgs(MgsArgs a) {
   }
 }
 
+// G (k x k, lower triangle used) of a block whose columns idx[0..nd) were zeroed: their rows and
+// columns become those of the identity, so the factorisation goes through and leaves them zero
+__global__ void k_patch_gram(Z* G, int k, const int* idx, int nd) {
+  const long long n = (long long)nd * k;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int d = idx[t / k], j = (int)(t % k);
+    const Z v = make_cuDoubleComplex(j == d ? 1.0 : 0.0, 0.0);
+    G[(size_t)j * k + d] = v;     // row d
+    G[(size_t)d * k + j] = v;     // column d
+  }
+}
+
+__global__ void k_diag_add(Z* G, int k, double shift) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x)
+    G[(size_t)i * k + i].x += shift;
+}
+
 // --------------------------- solver state ---------------------------
 struct Solver {
   cpw_b200_ctx* c;
@@ -282,7 +299,9 @@ struct Solver {
   int status = kOk;
   // wall-clock accounting per phase (printed when ipr > 1): 0 H|psi>, 1 Gram-Schmidt, 2 subspace eigensolve;
   // inside 1: 3 modified Gram-Schmidt leaves, 4 block passes against the converged vectors
-  double tphase[5] = {0, 0, 0, 0, 0};
+  // outside 0-2: 5 residual norms of the inner loop, 6 span test, 7 relaxation (without H|psi>),
+  // 8 Ritz subspace Hamiltonian, 9 Ritz rotations, copies and residual check
+  double tphase[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   long long n_gs = 0, n_gs_vec = 0, n_leaf = 0;
   bool timing = false;
   struct Tick {
@@ -295,12 +314,14 @@ struct Solver {
         t0 = std::chrono::steady_clock::now();
       }
     }
-    ~Tick() {
-      if (s->timing) {
+    void stop() {
+      if (s->timing && k >= 0) {
         cudaStreamSynchronize(s->st);
         s->tphase[k] += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
       }
+      k = -1;
     }
+    ~Tick() { stop(); }
   };
   const Z one = make_cuDoubleComplex(1, 0), zero = make_cuDoubleComplex(0, 0), mone = make_cuDoubleComplex(-1, 0);
 
@@ -394,15 +415,23 @@ struct Solver {
 
   // ---- Cholesky QR, twice: the in-block orthonormalisation of the mixed form ----
   // X <- X (L^H)^-1 with X^H X = L L^H, two passes. Before the first pass changes X, a
-  // failed factorisation or a pivot L_ii^2 below kCholDrop * xscl_i (near dependence, where
-  // the reference's drop rule may apply) sets *fallback and leaves X to the reference's
-  // recursive Gram-Schmidt.
+  // failed factorisation, a pivot L_ii^2 below 1e-20 xscl_i (a vector the reference's drop
+  // rule removes, grsch_mod_c16.f90) or below kCholCond G_ii (the block itself nearly
+  // dependent, beyond what Cholesky QR resolves) sets *fallback and leaves X to the
+  // reference's recursive Gram-Schmidt.
+  // Ritz subspace Hamiltonian reuse: the leading ham_clean columns of bas/hbas are unchanged
+  // since the last hbas^H bas, whose lower triangle (order ham_prev_n) is kept in ham_prev
+  int ham_clean = 0, ham_prev_n = 0;
+  long long ham_reused = 0, ham_full = 0;
+  DevBuf ham_prev;
+  void touch(int c0) { ham_clean = std::max(0, std::min(ham_clean, c0)); }
   bool chol = false;
   bool tc_rot = false;   // Ritz rotations on the tensor cores (mixed form with tensor-core projectors)
-  long long n_chol = 0, n_chol_fallback = 0;
-  DevBuf chol_g, chol_work, chol_info;
-  static constexpr double kCholDrop = 1e-12;
-  int cholqr(bool also, Z* x, Z* hx, int k, const double* xscl, bool* fallback) {
+  long long n_chol = 0, n_chol_fallback = 0, n_fb_info = 0, n_fb_drop = 0, n_fb_cond = 0;
+  DevBuf chol_g, chol_work, chol_info, chol_idx;
+  long long n_chol_dropped = 0, n_chol_shifted = 0;
+  static constexpr double kCholCond = 1e-12;
+  int cholqr(bool also, Z* x, Z* hx, int k, int* irow, const double* xscl, bool* fallback) {
     *fallback = false;
     if (k <= 0) return kOk;
     Tick tk(this, 3);
@@ -412,18 +441,63 @@ struct Solver {
       cusolverDnSetStream(sol, st);
     }
     int s;
-    if ((s = chol_g.ensure(sizeof(Z) * (size_t)k * k)) || (s = chol_info.ensure(sizeof(int)))) return s;
+    if ((s = chol_g.ensure(sizeof(Z) * (size_t)k * k)) || (s = chol_info.ensure(sizeof(int))) ||
+        (s = chol_idx.ensure(sizeof(int) * (size_t)k)))
+      return s;
     Z* G = (Z*)chol_g.p;
     int lw = 0;
     if (cusolverDnZpotrf_bufferSize(sol, CUBLAS_FILL_MODE_LOWER, k, G, k, &lw) != CUSOLVER_STATUS_SUCCESS)
       return fail(kCusolver, "zpotrf workspace");
     if ((s = chol_work.ensure(sizeof(Z) * (size_t)std::max(lw, 1)))) return s;
-    std::vector<Z> dg(k);
-    for (int pass = 0; pass < 2; ++pass) {
+    std::vector<Z> dg(k), dg0(k);
+    std::vector<int> dropped;
+    // two plain passes; when the first plain factorisation fails (a nearly dependent block),
+    // one shifted pass first (factor G + s I, s = 11 (m k + k (k + 1)) u trace(G), as in the
+    // published shifted Cholesky QR 3) brings the block to a condition Cholesky QR resolves
+    bool first = true, shift_now = false, shifted = false;
+    int done = 0;
+    while (done < 2) {
       {
         const double a1 = 1.0, b0 = 0.0;   // lower triangle of X^H X
         if (cublasZherk(blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, k, m, &a1, x, m, &b0, G, k) != CUBLAS_STATUS_SUCCESS)
           return fail(kCublas, "cholqr gram");
+      }
+      // squared norms of the block's vectors (the Gram diagonal, before the factorisation)
+      if ((s = ck(cudaMemcpy2DAsync(dg0.data(), sizeof(Z), G, sizeof(Z) * (size_t)(k + 1), sizeof(Z), k,
+                                    cudaMemcpyDeviceToHost, st),
+                  "cholqr norms")))
+        return s;
+      if (first || shift_now) {
+        if ((s = ck(cudaStreamSynchronize(st), "cholqr norms"))) return s;
+      }
+      if (first) {
+        // the reference's drop rule (grsch_mod_c16.f90: norm^2 below 1e-20 of the norm^2 before
+        // the passes against the converged vectors) removes vectors those passes reduced to
+        // rounding noise: zero and flag them
+        for (int i = 0; i < k; ++i)
+          if (!(dg0[i].x >= CEPS20 * xscl[i]) || !(xscl[i] > 0.0)) dropped.push_back(i);
+        for (int i : dropped) {
+          irow[i] = 0;
+          if ((s = ck(cudaMemsetAsync(x + (size_t)i * m, 0, sizeof(Z) * m, st), "cholqr drop")) ||
+              (also && (s = ck(cudaMemsetAsync(hx + (size_t)i * m, 0, sizeof(Z) * m, st), "cholqr drop"))))
+            return s;
+        }
+        if (!dropped.empty()) {
+          n_chol_dropped += (long long)dropped.size();
+          if ((s = ck(cudaMemcpyAsync(chol_idx.p, dropped.data(), sizeof(int) * dropped.size(),
+                                      cudaMemcpyHostToDevice, st),
+                      "cholqr drop")))
+            return s;
+        }
+      }
+      if (!dropped.empty())
+        k_patch_gram<<<std::max(1, std::min(1184, (int)((dropped.size() * k + 255) / 256))), 256, 0, st>>>(
+            G, k, (const int*)chol_idx.p, (int)dropped.size());
+      if (shift_now) {
+        double tr = 0.0;
+        for (int i = 0; i < k; ++i) tr += dg0[i].x;
+        const double sh = 11.0 * ((double)m * k + (double)k * (k + 1)) * 1.1102230246251565e-16 * tr;
+        k_diag_add<<<std::max(1, std::min(1184, (k + 255) / 256)), 256, 0, st>>>(G, k, sh);
       }
       if (cusolverDnZpotrf(sol, CUBLAS_FILL_MODE_LOWER, k, G, k, (Z*)chol_work.p, lw, (int*)chol_info.p) !=
           CUSOLVER_STATUS_SUCCESS)
@@ -435,11 +509,35 @@ struct Solver {
                   "cholqr diag")) ||
           (s = ck(cudaStreamSynchronize(st), "cholqr")))
         return s;
+      first = false;
       bool bad = info != 0;
-      for (int i = 0; i < k && !bad && pass == 0; ++i)
-        if (!(dg[i].x * dg[i].x > kCholDrop * xscl[i])) bad = true;
+      int why = bad ? 1 : 0;        // 1 factorisation, 2 drop rule, 3 conditioning
+      for (int i = 0; i < k && !bad && done == 0 && !shift_now; ++i) {
+        if (irow[i] == 0) continue;
+        const double piv = dg[i].x * dg[i].x;
+        if (!(piv > CEPS20 * xscl[i])) {
+          bad = true;
+          why = 2;
+        } else if (!(piv > kCholCond * dg0[i].x)) {
+          bad = true;
+          why = 3;
+        }
+      }
+      if (bad && done == 0 && !shifted && !shift_now) {
+        // X is unchanged: factor again with the shift
+        shift_now = true;
+        shifted = true;
+        ++n_chol_shifted;
+        continue;
+      }
+      if (bad && done == 0) {
+        if (why == 1) ++n_fb_info;
+        if (why == 2) ++n_fb_drop;
+        if (why == 3) ++n_fb_cond;
+      }
       if (bad) {
-        if (pass == 0) {
+        if (done == 0) {
+          // the zeroed vectors stay dropped; the recursive Gram-Schmidt takes the block
           *fallback = true;
           ++n_chol_fallback;
           return kOk;
@@ -452,6 +550,11 @@ struct Solver {
       if (also && cublasZtrsm(blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, CUBLAS_DIAG_NON_UNIT, m,
                               k, &one, G, k, hx, m) != CUBLAS_STATUS_SUCCESS)
         return fail(kCublas, "cholqr trsm");
+      if (shift_now) {
+        shift_now = false;      // the shifted pass conditions the block; two plain passes follow
+        continue;
+      }
+      ++done;
     }
     return kOk;
   }
@@ -578,7 +681,8 @@ struct Solver {
     }
     if (chol) {
       bool fb = false;
-      if (int s = cholqr(also, x + (size_t)nconv * m, also ? hx + (size_t)nconv * m : nullptr, k, xscl.data(), &fb))
+      if (int s = cholqr(also, x + (size_t)nconv * m, also ? hx + (size_t)nconv * m : nullptr, k, irow.data() + nconv,
+                         xscl.data(), &fb))
         return s;
       if (!fb) return kOk;
     }
@@ -860,7 +964,10 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
       // ---- ditsp_c16_loop ----
       lconv = false;
       lexit = false;
-      if ((s = S.rayleigh(nconv, niter, eg, work))) return s;
+      {
+        Solver::Tick tk5(&S, 5);
+        if ((s = S.rayleigh(nconv, niter, eg, work))) return s;
+      }
       const double xmold = xmax;
       xmax = 0.0;
       for (int n = nconv; n < std::min(ndeg, niter); ++n) xmax = std::max(xmax, work[n]);
@@ -921,6 +1028,7 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
       if (!lconv && !lexit && niter == nconv) lexit = true;
       if (!lconv && !lexit && ntst > nconv) {
         // span test against the previous basis vectors (ditsp_c16_loop.f90:396-461)
+        Solver::Tick tk6(&S, 6);
         const int k = ntst - nconv;
         if ((s = S.smallA.ensure(sizeof(Z) * (size_t)k * k))) return s;
         if ((s = S.gemm(CUBLAS_OP_C, CUBLAS_OP_N, k, k, mtxd, S.one, S.B(nexact + nconv), mtxd, PP + (size_t)nconv * mtxd,
@@ -964,6 +1072,7 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
       }
       if (!lconv && !lexit) {
         if (ntst > nconv) {
+          S.touch(nexact + nconv);
           if ((s = S.copycols(S.B(nexact + nconv), mtxd, PP + (size_t)nconv * mtxd, mtxd, ntst - nconv))) return s;
           std::vector<int> irowb;
           if ((s = S.grsch_loop(false, (Z*)S.bas.p, (Z*)S.hbas.p, nexact + nconv, nexact + ntst, irowb))) return s;
@@ -979,6 +1088,7 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
             compact_eg(ir2, nconv, niter);
           }
           const int nnew = ntst - ired - nconv;
+          S.touch(nexact + nconv);
           if ((s = S.hk(S.B(nexact + nconv), mtxd, S.HB(nexact + nconv), mtxd, nnew))) return s;
           nconv = ntst - ired;
           niter -= ired;
@@ -986,6 +1096,7 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
         // relaxation step
         const int nr = niter - nconv;
         if (nr > 0) {
+          Solver::Tick tk7(&S, 7);
           if ((s = S.dvec2.ensure(sizeof(double) * nr))) return s;
           if ((s = S.ck(cudaMemcpyAsync(S.dvec2.p, eg.data() + nconv, sizeof(double) * nr, cudaMemcpyHostToDevice, st),
                         "eg")))
@@ -999,6 +1110,7 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
           for (int i = 0; i < nr; ++i) sc[i] = 1.0 / sqrt(nrm[i].real());
           if ((s = S.colscale(PP + (size_t)nconv * mtxd, mtxd, nr, sc))) return s;
           lortho = false;
+          tk7.stop();
           if ((s = S.hk(PP + (size_t)nconv * mtxd, mtxd, HPP + (size_t)nconv * mtxd, mtxd, nr))) return s;
         }
       }
@@ -1011,7 +1123,10 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
     const int nlow = nexact + nitold - nconv;
     if (nsize > mxdsml) return fail(kBadArg, "ditsp_c16_ritz: change mxdsml");
     if (nconv < niter)
+    {
+      S.touch(nlow + nconv);
       if ((s = S.copycols(S.B(nlow + nconv), mtxd, PP + (size_t)nconv * mtxd, mtxd, niter - nconv))) return s;
+    }
     if (!lsafe || niter == nconv) {
       ++nsize;
       if (nsize > mxdsml) return fail(kBadArg, "ditsp_c16_ritz: change mxdsml");
@@ -1021,12 +1136,14 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
         const double xi = ran2(iseed);
         rv[k] = make_cuDoubleComplex(xr, xi);
       }
+      S.touch(nsize - 1);
       if ((s = S.ck(cudaMemcpyAsync(S.B(nsize - 1), rv.data(), sizeof(Z) * mtxd, cudaMemcpyHostToDevice, st), "ran")))
         return s;
       if ((s = S.ck(cudaStreamSynchronize(st), "ran"))) return s;
     }
     {
       std::vector<int> irowb;
+      S.touch(nexact + nconv);
       if ((s = S.grsch_loop(false, (Z*)S.bas.p, (Z*)S.hbas.p, nexact + nconv, nsize, irowb))) return s;
       int ired;
       if ((s = S.grsch_shift((Z*)S.bas.p, mtxd, nexact + nconv, nsize, irowb, &ired))) return s;
@@ -1034,15 +1151,45 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
     }
     if (nsize > mtxd) return fail(kBadArg, "ditsp_c16_ritz: problems with Gram-Schmidt");
     const int lo = nexact + nconv;
+    S.touch(lo);
     if ((s = S.hk(S.B(lo), mtxd, S.HB(lo), mtxd, nsize - lo))) return s;
     if ((s = S.smallV.ensure(sizeof(Z) * (size_t)nsize * nsize))) return s;
     // hamsm = hbas^H bas (ditsp_c16_ritz.f90:195); zheevd reads its lower triangle only, which
     // zherkx computes at half the cost of the full product
     {
+      Solver::Tick tk8(&S, 8);
       const double b0 = 0.0;
-      if (cublasZherkx(S.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, nsize, mtxd, &S.one, (Z*)S.hbas.p, mtxd,
-                       (Z*)S.bas.p, mtxd, &b0, (Z*)S.smallV.p, nsize) != CUBLAS_STATUS_SUCCESS)
-        return fail(kCublas, "ritz hamsm");
+      Z* H = (Z*)S.smallV.p;
+      // the leading block over columns untouched since the previous Ritz step is that step's
+      // (the same products); only the rows of the new columns are computed
+      const int c = std::min(S.ham_clean, std::min(S.ham_prev_n, nsize));
+      if (c > 0) {
+        ++S.ham_reused;
+        if ((s = S.ck(cudaMemcpy2DAsync(H, sizeof(Z) * (size_t)nsize, S.ham_prev.p, sizeof(Z) * (size_t)S.ham_prev_n,
+                                        sizeof(Z) * (size_t)c, c, cudaMemcpyDeviceToDevice, st),
+                      "ritz hamsm reuse")))
+          return s;
+        if (c < nsize) {
+          if ((s = S.gemm(CUBLAS_OP_C, CUBLAS_OP_N, nsize - c, c, mtxd, S.one, S.HB(c), mtxd, S.B(0), mtxd, S.zero,
+                          H + c, nsize, "ritz hamsm rows")))
+            return s;
+          if (cublasZherkx(S.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, nsize - c, mtxd, &S.one, S.HB(c), mtxd, S.B(c),
+                           mtxd, &b0, H + (size_t)c * nsize + c, nsize) != CUBLAS_STATUS_SUCCESS)
+            return fail(kCublas, "ritz hamsm");
+        }
+      } else {
+        ++S.ham_full;
+        if (cublasZherkx(S.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, nsize, mtxd, &S.one, (Z*)S.hbas.p, mtxd,
+                         (Z*)S.bas.p, mtxd, &b0, H, nsize) != CUBLAS_STATUS_SUCCESS)
+          return fail(kCublas, "ritz hamsm");
+      }
+      // keep it for the next Ritz step (zheevd overwrites smallV)
+      if ((s = S.ham_prev.ensure(sizeof(Z) * (size_t)nsize * nsize)) ||
+          (s = S.ck(cudaMemcpyAsync(S.ham_prev.p, H, sizeof(Z) * (size_t)nsize * nsize, cudaMemcpyDeviceToDevice, st),
+                    "ritz hamsm keep")))
+        return s;
+      S.ham_prev_n = nsize;
+      S.ham_clean = nsize;
     }
     std::vector<double> egs;
     if ((s = S.diag((Z*)S.smallV.p, nsize, egs))) return s;
@@ -1095,6 +1242,7 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
     }
     // psi = bas V, hpsi = hbas V (ditsp_c16_ritz.f90:284-287): split-TF32 tensor-core products in the
     // mixed form (V and the subspace Hamiltonian stay FP64), FP64 ZGEMM otherwise
+    Solver::Tick tk9(&S, 9);
     if (S.tc_rot) {
       if ((s = tc_zgemm_nn(c, mtxd, niter, nsize, S.bas.p, mtxd, S.smallV.p, nsize, PP, mtxd, st)) ||
           (s = tc_zgemm_nn(c, mtxd, niter, nsize, S.hbas.p, mtxd, S.smallV.p, nsize, HPP, mtxd, st)))
@@ -1108,12 +1256,14 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
         return s;
     }
     if (niter > nconv) {
+      S.touch(nexact + nconv);
       if ((s = S.copycols(S.B(nexact + nconv), mtxd, PP + (size_t)nconv * mtxd, mtxd, niter - nconv))) return s;
       if ((s = S.copycols(S.HB(nexact + nconv), mtxd, HPP + (size_t)nconv * mtxd, mtxd, niter - nconv))) return s;
     }
     if (nconv >= ndeg) neig = ndeg;
     xmax = S.xmax_error(neig);
     if (xmax < 0) return fail(kCuda, "ditsp_c16: residual evaluation failed");
+    tk9.stop();
     if (itlog && ic <= itlog_rows) {
       // iteration log row: elapsed s, xmax, nconv, H|psi> products so far, eg(1:mxdbnd)
       double* row = itlog + (size_t)(ic - 1) * (4 + mxdbnd);
@@ -1156,8 +1306,13 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
            "subspace eigensolve %.4f s, other %.4f s\n",
            S.ihk, tot, S.tphase[0], S.tphase[1], S.tphase[2], tot - S.tphase[0] - S.tphase[1] - S.tphase[2]);
     printf("  ditsp_c16: Gram-Schmidt %lld calls, %lld vectors: passes against converged %.4f s, "
-           "in-block %.4f s (%lld modified Gram-Schmidt leaves, %lld Cholesky QR, %lld fallbacks)\n",
-           S.n_gs, S.n_gs_vec, S.tphase[4], S.tphase[3], S.n_leaf, S.n_chol, S.n_chol_fallback);
+           "in-block %.4f s (%lld modified Gram-Schmidt leaves, %lld Cholesky QR dropping %lld vectors, %lld shifted, "
+           "%lld fallbacks: %lld factorisation, %lld drop rule, %lld conditioning)\n",
+           S.n_gs, S.n_gs_vec, S.tphase[4], S.tphase[3], S.n_leaf, S.n_chol, S.n_chol_dropped, S.n_chol_shifted,
+           S.n_chol_fallback, S.n_fb_info, S.n_fb_drop, S.n_fb_cond);
+    printf("  ditsp_c16: outside: residual norms %.4f s, span test %.4f s, relaxation %.4f s, Ritz subspace "
+           "Hamiltonian %.4f s (%lld reused leading blocks, %lld full), Ritz rotations + residual check %.4f s\n",
+           S.tphase[5], S.tphase[6], S.tphase[7], S.tphase[8], S.ham_reused, S.ham_full, S.tphase[9]);
     fflush(stdout);
   }
   if (S.sol) cusolverDnDestroy(S.sol);
