@@ -3,6 +3,7 @@
 // GEMMs of Src/cpw_lib/hk_psi_nl_c16.f90:82-97).
 #include <math.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -123,8 +124,9 @@ int plan_for_box(cpw_b200_ctx* c, const int kd[3], const int* kmscr, LocalPlan* 
   while (p.tcol > 4 && esz * ((size_t)p.ny * p.rowp + (size_t)p.n2 * p.tcol + n1 + n2) > cmax) p.tcol /= 2;
   if (esz * ((size_t)p.ny * p.rowp + (size_t)p.n2 * p.tcol + n1 + n2) > cmax)
     return fail(kUnsupported, "set_basis: plane does not fit in shared memory");
-  p.cb = 32;
-  while (p.cb > 4 && esz * ((size_t)n3 * p.cb + n3) > cmax) p.cb /= 2;
+  int smsm = 0;
+  cudaDeviceGetAttribute(&smsm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
+  p.cb = column_tile(esz, p, cmax, (size_t)smsm);
   *out = p;
   return kOk;
 }

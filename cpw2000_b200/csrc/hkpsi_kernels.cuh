@@ -246,7 +246,7 @@ template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile(
 
 // shared memory of k_z_vloc_pipe: work columns, two staging buffers of kept planes, twiddles, V tile
 template <typename T> inline size_t smem_columns_pipe(const LocalPlan& p, int cb) {
-  return sizeof(C2<T>) * ((size_t)p.n3 * cb + 2 * (size_t)p.nz * cb + p.n3) + sizeof(T) * (size_t)p.n3 * cb;
+  return smem_columns_pipe_bytes(sizeof(C2<T>), p, cb);
 }
 
 template <typename T, int RZ1, int RZ2, int CB>

@@ -17,6 +17,8 @@ CPWB_DECLARE(float, 5, 8, 5, 8, 5, 8, 32, 32)
 CPWB_DECLARE(double, 8, 12, 8, 12, 8, 12, 32, 32)
 CPWB_DECLARE(float, 8, 12, 8, 12, 8, 12, 32, 32)
 CPWB_DECLARE(double, 12, 12, 12, 12, 12, 12, 32, 32)
+CPWB_DECLARE(double, 12, 12, 12, 12, 12, 12, 32, 16)
+CPWB_DECLARE(float, 12, 12, 12, 12, 12, 12, 32, 16)
 CPWB_DECLARE(float, 12, 12, 12, 12, 12, 12, 32, 32)
 CPWB_DECLARE(double, 0, 0, 0, 0, 0, 0, 0, 0)
 CPWB_DECLARE(float, 0, 0, 0, 0, 0, 0, 0, 0)
@@ -26,6 +28,10 @@ static bool is_split(const FftDim& d, int r1, int r2) { return d.r1 == r1 && d.r
 
 template <typename T>
 cudaError_t launch_local(CPWB_LAUNCH_ARGS(T)) {
+  // 144^3 with the z stage in 16-column tiles
+  if (p.n1 == p.n2 && p.n2 == p.n3 && p.tcol == 32 && p.cb == 16 && is_split(p.dx, 12, 12))
+    return kern::launch_impl<T, 12, 12, 12, 12, 12, 12, 32, 16>(p, nbc, band0, psi, ldpsi, hpsi, ldh, plane_start,
+                                                               pw_idx, pw_pos, ekpg, vr, twx, twy, twz, W, st, ev);
   const bool cubic = p.n1 == p.n2 && p.n2 == p.n3 && p.tcol == 32 && p.cb == 32;
   if (cubic && is_split(p.dx, 8, 12))
     return kern::launch_impl<T, 8, 12, 8, 12, 8, 12, 32, 32>(p, nbc, band0, psi, ldpsi, hpsi, ldh, plane_start,

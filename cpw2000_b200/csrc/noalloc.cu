@@ -218,8 +218,9 @@ extern "C" int cpw_b200_hk_psi_loc_noalloc(int mtxd, int neig, const void* psi, 
   while (p.tcol > 4 && es * ((size_t)p.ny * p.rowp + (size_t)n2 * p.tcol + n1 + n2) > (size_t)smax) p.tcol /= 2;
   if (es * ((size_t)p.ny * p.rowp + (size_t)n2 * p.tcol + n1 + n2) > (size_t)smax)
     return fail(kUnsupported, "hk_psi_loc_noalloc: plane does not fit in shared memory");
-  p.cb = 32;
-  while (p.cb > 4 && es * ((size_t)n3 * p.cb + n3) > (size_t)smax) p.cb /= 2;
+  int smsm = 0;
+  cudaDeviceGetAttribute(&smsm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  p.cb = column_tile(es, p, (size_t)smax, (size_t)smsm);
 
   const size_t per_band = es * (size_t)p.nz * (size_t)p.plane;
   const size_t room = kNoAllocScratchBytes - off_slab;
