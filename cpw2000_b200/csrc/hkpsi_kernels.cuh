@@ -15,14 +15,23 @@ namespace kern {
 
 constexpr int kThreadsPlanes = 256;
 constexpr int kThreadsCols = 256;
+// Threads of a CTA of a two-pass (four-step) transform stage: one per line of the larger pass
+// when that is 192 or 384 lines (96- and 144-point lines in 32- or 16-column tiles), so that
+// no pass leaves part of the CTA idle before the barrier; else 256.
+constexpr int pass_threads(int lines_a, int lines_b) {
+  return (lines_a > lines_b ? lines_a : lines_b) == 384 ? 384
+         : (lines_a > lines_b ? lines_a : lines_b) == 192 ? 192 : 256;
+}
+// CTAs per SM asked of the register allocator: two CTAs of 384 threads fit in 80 registers.
+constexpr int pass_min_blocks(int nt) { return nt == 384 ? 2 : 1; }
 
 template <typename T> __device__ __forceinline__ C2<T> czero() { return mk<T>(T(0), T(0)); }
 
 // ---------------------------------------------------------------------------
 // A: scatter + inverse x + inverse y, one CTA per (band, kept z-plane)
 // ---------------------------------------------------------------------------
-template <typename T, int RX1, int RX2, int RY1, int RY2, int TC>
-__global__ void __launch_bounds__(kThreadsPlanes, 1)
+template <typename T, int RX1, int RX2, int RY1, int RY2, int TC, int NT = kThreadsPlanes>
+__global__ void __launch_bounds__(NT, pass_min_blocks(NT))
 k_inv_xy(LocalPlan p, int band0, const C2<double>* __restrict__ psi, long long ldpsi,
          const int* __restrict__ plane_start, const int* __restrict__ pw_idx,
          const int* __restrict__ pw_pos, const C2<T>* __restrict__ twx,
@@ -249,8 +258,8 @@ template <typename T> inline size_t smem_columns_pipe(const LocalPlan& p, int cb
   return smem_columns_pipe_bytes(sizeof(C2<T>), p, cb);
 }
 
-template <typename T, int RZ1, int RZ2, int CB>
-__global__ void __launch_bounds__(kThreadsCols, 1)
+template <typename T, int RZ1, int RZ2, int CB, int NT = kThreadsCols>
+__global__ void __launch_bounds__(NT, pass_min_blocks(NT))
 k_z_vloc_pipe(LocalPlan p, int nbc, int bands_per_group, const T* __restrict__ vr, const C2<T>* __restrict__ twz,
               C2<T>* __restrict__ W) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -361,8 +370,8 @@ k_z_vloc_pipe(LocalPlan p, int nbc, int bands_per_group, const T* __restrict__ v
 // ---------------------------------------------------------------------------
 // C: forward y + forward x + gather + kinetic, one CTA per (band, kept z-plane)
 // ---------------------------------------------------------------------------
-template <typename T, int RX1, int RX2, int RY1, int RY2, int TC>
-__global__ void __launch_bounds__(kThreadsPlanes, 1)
+template <typename T, int RX1, int RX2, int RY1, int RY2, int TC, int NT = kThreadsPlanes>
+__global__ void __launch_bounds__(NT, pass_min_blocks(NT))
 k_fwd_xy(LocalPlan p, int band0, const C2<double>* __restrict__ psi, long long ldpsi,
          C2<double>* __restrict__ hpsi, long long ldh, const int* __restrict__ plane_start,
          const int* __restrict__ pw_idx, const int* __restrict__ pw_pos,
@@ -495,9 +504,15 @@ cudaError_t launch_impl(const LocalPlan& p, int nbc, int band0, const C2<double>
                         C2<double>* hpsi, long long ldh, const int* plane_start, const int* pw_idx,
                         const int* pw_pos, const double* ekpg, const T* vr, const C2<T>* twx, const C2<T>* twy,
                         const C2<T>* twz, C2<T>* W, cudaStream_t st, cudaEvent_t* ev) {
+  constexpr int NTP = TC && RY1 ? pass_threads(TC * RY2, TC * RY1) : kThreadsPlanes;
+  constexpr int NTZ = CB && RZ1 ? pass_threads(CB * RZ2, CB * RZ1) : kThreadsCols;
+  // C keeps 256 threads where 384 measured slower: FP64 on 144-point lines (the 80-register
+  // cap spills) and FP32 on 96-point lines.
+  constexpr bool c_wide = sizeof(T) == 8 ? RY1 * RY2 < 128 : RY1 * RY2 >= 128;
+  constexpr int NTC = NTP == 384 && c_wide ? 384 : kThreadsPlanes;
   const size_t sm_pl = smem_planes<T>(p);
-  auto* ka = k_inv_xy<T, RX1, RX2, RY1, RY2, TC>;
-  auto* kc = k_fwd_xy<T, RX1, RX2, RY1, RY2, TC>;
+  auto* ka = k_inv_xy<T, RX1, RX2, RY1, RY2, TC, NTP>;
+  auto* kc = k_fwd_xy<T, RX1, RX2, RY1, RY2, TC, NTC>;
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pl)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pl)) != cudaSuccess) return e;
@@ -507,7 +522,7 @@ cudaError_t launch_impl(const LocalPlan& p, int nbc, int band0, const C2<double>
   cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   dim3 gA(p.nz, nbc);
   if (ev) cudaEventRecord(ev[0], st);
-  ka<<<gA, kThreadsPlanes, sm_pl, st>>>(p, band0, psi, ldpsi, plane_start, pw_idx, pw_pos, twx, twy, W);
+  ka<<<gA, NTP, sm_pl, st>>>(p, band0, psi, ldpsi, plane_start, pw_idx, pw_pos, twx, twy, W);
   if (ev) cudaEventRecord(ev[1], st);
   const size_t sm_pipe = smem_columns_pipe<T>(p, p.cb);
   const long long tiles = (p.plane + p.cb - 1) / p.cb;
@@ -523,14 +538,13 @@ cudaError_t launch_impl(const LocalPlan& p, int nbc, int band0, const C2<double>
     long long groups = std::max(1LL, std::min((long long)nbc, (per_sm * nsm + tiles - 1) / tiles));
     const int per = (int)((nbc + groups - 1) / groups);
     groups = (nbc + per - 1) / per;
-    auto* kbp = k_z_vloc_pipe<T, RZ1, RZ2, CB>;
+    auto* kbp = k_z_vloc_pipe<T, RZ1, RZ2, CB, NTZ>;
     if ((e = cudaFuncSetAttribute(kbp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pipe)) != cudaSuccess)
       return e;
-    kbp<<<dim3((unsigned)tiles, (unsigned)groups), kThreadsCols, sm_pipe, st>>>(p, nbc, per, vr, twz, W);
+    kbp<<<dim3((unsigned)tiles, (unsigned)groups), NTZ, sm_pipe, st>>>(p, nbc, per, vr, twz, W);
   }
   if (ev) cudaEventRecord(ev[2], st);
-  kc<<<gA, kThreadsPlanes, sm_pl, st>>>(p, band0, psi, ldpsi, hpsi, ldh, plane_start, pw_idx, pw_pos, ekpg, twx,
-                                        twy, W);
+  kc<<<gA, NTC, sm_pl, st>>>(p, band0, psi, ldpsi, hpsi, ldh, plane_start, pw_idx, pw_pos, ekpg, twx, twy, W);
   if (ev) cudaEventRecord(ev[3], st);
   return cudaGetLastError();
 }
@@ -540,11 +554,12 @@ template <typename T, int RX1, int RX2, int RY1, int RY2, int TC>
 cudaError_t launch_inv_impl(const LocalPlan& p, int nbc, int band0, const C2<double>* psi, long long ldpsi,
                             const int* plane_start, const int* pw_idx, const int* pw_pos, const C2<T>* twx,
                             const C2<T>* twy, C2<T>* W, cudaStream_t st) {
+  constexpr int NTP = TC && RY1 ? pass_threads(TC * RY2, TC * RY1) : kThreadsPlanes;
   const size_t sm_pl = smem_planes<T>(p);
-  auto* ka = k_inv_xy<T, RX1, RX2, RY1, RY2, TC>;
+  auto* ka = k_inv_xy<T, RX1, RX2, RY1, RY2, TC, NTP>;
   cudaError_t e = cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pl);
   if (e != cudaSuccess) return e;
-  ka<<<dim3(p.nz, nbc), kThreadsPlanes, sm_pl, st>>>(p, band0, psi, ldpsi, plane_start, pw_idx, pw_pos, twx, twy, W);
+  ka<<<dim3(p.nz, nbc), NTP, sm_pl, st>>>(p, band0, psi, ldpsi, plane_start, pw_idx, pw_pos, twx, twy, W);
   return cudaGetLastError();
 }
 
