@@ -49,11 +49,6 @@ k_inv_xy(LocalPlan p, int band0, const C2<double>* __restrict__ psi, long long l
   const int zi = blockIdx.x, b = blockIdx.y;
   const int tid = threadIdx.x, nt = blockDim.x;
 
-  for (int i = tid; i < n1; i += nt) sx[i] = twx[i];
-  for (int i = tid; i < n2; i += nt) sy[i] = twy[i];
-  for (int i = tid; i < ny * rowp; i += nt) R[i] = czero<T>();
-  __syncthreads();
-
   const C2<double>* ps = psi + (size_t)(band0 + b) * ldpsi;
   if (p.kdesc) {      // batch of k-points: this band's own basis and block
     const int2 r = p.bref[band0 + b];
@@ -64,7 +59,29 @@ k_inv_xy(LocalPlan p, int band0, const C2<double>* __restrict__ psi, long long l
     pw_pos = D.pw_pos;
   }
   const int e0 = plane_start[zi], e1 = plane_start[zi + 1];
-  for (int e = e0 + tid; e < e1; e += nt) {
+  // the first kPre sphere points of this thread are loaded before the plane is cleared, so
+  // that their gather latency overlaps the clearing
+  constexpr int kPre = 2;
+  int pre_pos[kPre];
+  C2<double> pre_v[kPre];
+#pragma unroll
+  for (int j = 0; j < kPre; ++j) {
+    const int e = e0 + tid + j * nt;
+    pre_pos[j] = -1;
+    if (e < e1) {
+      pre_pos[j] = pw_pos[e];
+      pre_v[j] = ps[pw_idx[e]];
+    }
+  }
+  for (int i = tid; i < n1; i += nt) sx[i] = twx[i];
+  for (int i = tid; i < n2; i += nt) sy[i] = twy[i];
+  for (int i = tid; i < ny * rowp; i += nt) R[i] = czero<T>();
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < kPre; ++j)
+    if (pre_pos[j] >= 0)
+      R[(pre_pos[j] >> 16) * rowp + (pre_pos[j] & 0xffff)] = mk<T>(T(pre_v[j].x), T(pre_v[j].y));
+  for (int e = e0 + tid + kPre * nt; e < e1; e += nt) {
     const int pos = pw_pos[e];
     const C2<double> v = ps[pw_idx[e]];
     R[(pos >> 16) * rowp + (pos & 0xffff)] = mk<T>(T(v.x), T(v.y));
@@ -395,10 +412,13 @@ k_fwd_xy(LocalPlan p, int band0, const C2<double>* __restrict__ psi, long long l
   const C2<T>* Wp = W + ((size_t)b * p.nz + zi) * (size_t)p.plane;
   for (int xb = 0; xb < n1; xb += tc) {
     const int ncol = min(tc, n1 - xb);
+    // the tile's columns of every y row, all copies in flight at once
     for (int it = tid; it < tc * n2; it += nt) {
       const int xl = it % tc, y = it / tc;
-      if (xl < ncol) Tb[(size_t)y * tc + xl] = Wp[(size_t)y * n1 + xb + xl];
+      if (xl < ncol) cp_async_bytes(Tb + (size_t)y * tc + xl, Wp + (size_t)y * n1 + xb + xl, (int)sizeof(C2<T>));
     }
+    cp_async_commit();
+    cp_async_wait<0>();
     __syncthreads();
     for (int it = tid; it < tc * r2y; it += nt) {
       const int xl = it % tc, n2i = it / tc;
