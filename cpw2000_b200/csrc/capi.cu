@@ -91,7 +91,7 @@ struct DropinPipe {
 };
 
 int dropin_stage_in(cpw_b200_ctx* c, int m, int nb, const double* psi, long long ldh_host, DropinPipe* pp) {
-  int kChunks = 4;
+  int kChunks = 6;
   constexpr int kMinChunk = 16;
   if (const char* v = getenv("CPW_B200_DROPIN_CHUNKS")) kChunks = std::max(1, atoi(v));
   DropinPipe& p = *pp;
@@ -130,17 +130,68 @@ int dropin_wait(cpw_b200_ctx* c) {
   return kOk;
 }
 
+// FP64 projector products of a chunked call: P_k = X^H psi_k of every chunk on the projection
+// stream as soon as the chunk's copy landed (it needs psi_k only), so that the compute stream
+// runs the local kernels of chunk k and then only the expansion Hpsi_k += (X D) P_k. A 40-band
+// ZGEMM is much less efficient than a 160-band one; this takes the projections off the path.
+int dropin_nl_setup(cpw_b200_ctx* c, const DropinPipe& p) {
+  cudaError_t e;
+  if (!c->s_nl && (e = cudaStreamCreateWithFlags(&c->s_nl, cudaStreamNonBlocking)) != cudaSuccess)
+    return cuda_fail(e, "hk_psi_c16 stream");
+  if (!c->blas_nl) {
+    if (cublasCreate(&c->blas_nl) != CUBLAS_STATUS_SUCCESS) {
+      c->blas_nl = nullptr;
+      return fail(kCublas, "cublasCreate failed");
+    }
+    cublasSetPointerMode(c->blas_nl, CUBLAS_POINTER_MODE_HOST);
+  }
+  while ((int)c->ev_nl.size() < p.nchunk) {
+    cudaEvent_t ev;
+    if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return cuda_fail(e, "event");
+    c->ev_nl.push_back(ev);
+  }
+  return c->proj.ensure((size_t)c->nanl * p.nb * sizeof(C2d));
+}
+
 int dropin_compute_out(cpw_b200_ctx* c, const DropinPipe& p, double* hpsi, bool wait = true) {
   cudaError_t e;
   const int m = p.m;
   C2d* din = (C2d*)c->h_in.p;
   C2d* dout = (C2d*)c->h_out.p;
+  const bool split_nl = p.nchunk > 1 && c->nanl > 0 && !(c->precision == 2 && c->tc_ready);
+  if (split_nl) {
+    if (int s = dropin_nl_setup(c, p)) return s;
+    // the projection stream starts after earlier work on the compute stream (proj reuse)
+    cudaEvent_t start = c->ev_pipe[2 * p.nchunk];
+    if ((e = cudaEventRecord(start, c->stream)) != cudaSuccess || (e = cudaStreamWaitEvent(c->s_nl, start, 0)) != cudaSuccess)
+      return cuda_fail(e, "hk_psi_c16 pipeline");
+  }
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
   for (int k = 0; k < p.nchunk; ++k) {
     const int b0 = k * p.chunk, nbc = std::min(p.chunk, p.nb - b0);
     cudaEvent_t in_done = c->ev_pipe[2 * k], out_ready = c->ev_pipe[2 * k + 1];
     if ((e = cudaStreamWaitEvent(c->stream, in_done, 0)) != cudaSuccess) return cuda_fail(e, "hk_psi_c16 pipeline");
-    if (int s = ctx_hkpsi_device(c, nbc, din + (size_t)b0 * m, m, dout + (size_t)b0 * m, m, c->stream, true, true))
+    if (split_nl) {
+      cuDoubleComplex* pk = (cuDoubleComplex*)c->proj.p + (size_t)b0 * c->nanl;
+      if ((e = cudaStreamWaitEvent(c->s_nl, in_done, 0)) != cudaSuccess) return cuda_fail(e, "hk_psi_c16 pipeline");
+      cublasSetStream(c->blas_nl, c->s_nl);
+      // P_k = X^H psi_k (hk_psi_nl_c16.f90:82)
+      if (cublasZgemm(c->blas_nl, CUBLAS_OP_C, CUBLAS_OP_N, c->nanl, nbc, m, &one, (const cuDoubleComplex*)c->anl.p, m,
+                      (const cuDoubleComplex*)(din + (size_t)b0 * m), m, &zero, pk, c->nanl) != CUBLAS_STATUS_SUCCESS)
+        return fail(kCublas, "hk_psi_c16: zgemm X^H psi");
+      if ((e = cudaEventRecord(c->ev_nl[k], c->s_nl)) != cudaSuccess) return cuda_fail(e, "hk_psi_c16 pipeline");
+      if (int s = ctx_hkpsi_device(c, nbc, din + (size_t)b0 * m, m, dout + (size_t)b0 * m, m, c->stream, true, false))
+        return s;
+      if ((e = cudaStreamWaitEvent(c->stream, c->ev_nl[k], 0)) != cudaSuccess) return cuda_fail(e, "hk_psi_c16 pipeline");
+      cublasSetStream(c->blas, c->stream);
+      // Hpsi_k += (X D) P_k (hk_psi_nl_c16.f90:87-96)
+      if (cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, m, nbc, c->nanl, &one, (const cuDoubleComplex*)c->anld.p, m,
+                      pk, c->nanl, &one, (cuDoubleComplex*)(dout + (size_t)b0 * m), m) != CUBLAS_STATUS_SUCCESS)
+        return fail(kCublas, "hk_psi_c16: zgemm X D P");
+    } else if (int s = ctx_hkpsi_device(c, nbc, din + (size_t)b0 * m, m, dout + (size_t)b0 * m, m, c->stream, true,
+                                        true)) {
       return s;
+    }
     if ((e = cudaEventRecord(out_ready, c->stream)) != cudaSuccess || (e = cudaStreamWaitEvent(c->s_out, out_ready, 0)) != cudaSuccess)
       return cuda_fail(e, "hk_psi_c16 pipeline");
     if (int s = d2h_cols(hpsi + 2 * (size_t)b0 * p.ldh, p.ldh, dout + (size_t)b0 * m, m, m, nbc, c->s_out)) return s;
@@ -242,9 +293,13 @@ int cpw_b200_destroy(cpw_b200_ctx* c) {
   cudaStreamSynchronize(c->stream);
   if (c->s_in) cudaStreamSynchronize(c->s_in);
   if (c->s_out) cudaStreamSynchronize(c->s_out);
+  if (c->s_nl) cudaStreamSynchronize(c->s_nl);
   for (cudaEvent_t e : c->ev_pipe) cudaEventDestroy(e);
+  for (cudaEvent_t e : c->ev_nl) cudaEventDestroy(e);
   if (c->s_in) cudaStreamDestroy(c->s_in);
   if (c->s_out) cudaStreamDestroy(c->s_out);
+  if (c->blas_nl) cublasDestroy(c->blas_nl);
+  if (c->s_nl) cudaStreamDestroy(c->s_nl);
   if (c->blas) cublasDestroy(c->blas);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;

@@ -95,6 +95,11 @@ struct cpw_b200_ctx {
   // drop-in host path: copy streams and per-chunk events of the pipelined transfer
   cudaStream_t s_in = nullptr, s_out = nullptr;
   std::vector<cudaEvent_t> ev_pipe;
+  // drop-in host path, FP64 projectors: projections of the band chunks on their own stream
+  // and cuBLAS handle (own workspace), so that they leave the chunk's critical path
+  cudaStream_t s_nl = nullptr;
+  cublasHandle_t blas_nl = nullptr;
+  std::vector<cudaEvent_t> ev_nl;
   cublasHandle_t blas = nullptr;
   int precision = 0;            // 0: FP64; 1: FP32 local + FP64 projector GEMMs; 2: 1 with split-TF32 tensor-core projectors
   size_t slab_budget = 512ull << 20;

@@ -408,6 +408,19 @@ k_fwd_xy(LocalPlan p, int band0, const C2<double>* __restrict__ psi, long long l
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int i = tid; i < n1; i += nt) sx[i] = twx[i];
   for (int i = tid; i < n2; i += nt) sy[i] = twy[i];
+  const C2<double>* ps = psi + (size_t)(band0 + b) * ldpsi;
+  C2<double>* hp = hpsi + (size_t)(band0 + b) * ldh;
+  if (p.kdesc) {      // batch of k-points: this band's own basis and block
+    const int2 r = p.bref[band0 + b];
+    const KDesc& D = p.kdesc[r.x];
+    ps = D.psi + (size_t)r.y * D.ldpsi;
+    hp = D.hpsi + (size_t)r.y * D.ldh;
+    plane_start = D.plane_start;
+    pw_idx = D.pw_idx;
+    pw_pos = D.pw_pos;
+    ekpg = D.ekpg;
+  }
+  const int e0 = plane_start[zi], e1 = plane_start[zi + 1];
 
   const C2<T>* Wp = W + ((size_t)b * p.nz + zi) * (size_t)p.plane;
   for (int xb = 0; xb < n1; xb += tc) {
@@ -418,6 +431,16 @@ k_fwd_xy(LocalPlan p, int band0, const C2<double>* __restrict__ psi, long long l
       if (xl < ncol) cp_async_bytes(Tb + (size_t)y * tc + xl, Wp + (size_t)y * n1 + xb + xl, (int)sizeof(C2<T>));
     }
     cp_async_commit();
+    if (sizeof(T) == 8 && xb == 0 && ekpg) {
+      // while the first tile lands: bring the psi values and kinetic terms of the final gather
+      // into L2, so that its dependent loads do not wait on HBM at the end of the CTA (FP64
+      // only: in FP32 the extra registers cost a CTA per SM on 96-point lines)
+      for (int e = e0 + tid; e < e1; e += nt) {
+        const int i = pw_idx[e];
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(ps + i));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(ekpg + i));
+      }
+    }
     cp_async_wait<0>();
     __syncthreads();
     for (int it = tid; it < tc * r2y; it += nt) {
@@ -487,19 +510,6 @@ k_fwd_xy(LocalPlan p, int band0, const C2<double>* __restrict__ psi, long long l
   __syncthreads();
 
   // gather the sphere (permuted x storage) and add the kinetic diagonal
-  const C2<double>* ps = psi + (size_t)(band0 + b) * ldpsi;
-  C2<double>* hp = hpsi + (size_t)(band0 + b) * ldh;
-  if (p.kdesc) {      // batch of k-points: this band's own basis and block
-    const int2 r = p.bref[band0 + b];
-    const KDesc& D = p.kdesc[r.x];
-    ps = D.psi + (size_t)r.y * D.ldpsi;
-    hp = D.hpsi + (size_t)r.y * D.ldh;
-    plane_start = D.plane_start;
-    pw_idx = D.pw_idx;
-    pw_pos = D.pw_pos;
-    ekpg = D.ekpg;
-  }
-  const int e0 = plane_start[zi], e1 = plane_start[zi + 1];
   for (int e = e0 + tid; e < e1; e += nt) {
     const int pos = pw_pos[e];
     const int x = pos & 0xffff, yi = pos >> 16;
