@@ -46,6 +46,37 @@ template <> struct K<float> {
   __device__ __forceinline__ float mul(float x) const { return fmaf(x, h, x * l); }
 };
 template <typename T> __device__ __forceinline__ C2<T> kscal(C2<T> a, K<T> k) { return mk<T>(k.mul(a.x), k.mul(a.y)); }
+
+// FP32 complex add, subtract and split-constant scaling as packed two-lane instructions
+// (add/sub/mul/fma .rn.f32x2, sm_100): the same per-component IEEE rounding as the scalar
+// forms above, half the instructions in the butterflies of the issue-bound FP32 transforms.
+__device__ __forceinline__ unsigned long long f32x2_bits(C2<float> a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+__device__ __forceinline__ C2<float> f32x2_val(unsigned long long r) {
+  C2<float> a;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+  return a;
+}
+__device__ __forceinline__ C2<float> operator+(C2<float> a, C2<float> b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f32x2_bits(a)), "l"(f32x2_bits(b)));
+  return f32x2_val(d);
+}
+__device__ __forceinline__ C2<float> operator-(C2<float> a, C2<float> b) {
+  unsigned long long d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f32x2_bits(a)), "l"(f32x2_bits(b)));
+  return f32x2_val(d);
+}
+template <> __device__ __forceinline__ C2<float> kscal<float>(C2<float> a, K<float> k) {
+  unsigned long long t, d;
+  const unsigned long long x = f32x2_bits(a);
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(t) : "l"(x), "l"(f32x2_bits(mk<float>(k.l, k.l))));
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(x), "l"(f32x2_bits(mk<float>(k.h, k.h))), "l"(t));
+  return f32x2_val(d);
+}
 // a * (c + i s) with split constants
 __device__ __forceinline__ C2<double> kcmul(C2<double> a, K<double> c, K<double> s) {
   return mk<double>(a.x * c.v - a.y * s.v, a.x * s.v + a.y * c.v);
