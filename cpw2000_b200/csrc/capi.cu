@@ -392,6 +392,16 @@ int cpw_b200_set_projectors_device(cpw_b200_ctx* c, int nanl, const void* anlga,
   return ctx_set_projectors(c, nanl, (const double*)anlga, ld, (const double*)xnlkb, true);
 }
 
+int cpw_b200_proj_nl_kb_device(cpw_b200_ctx* c, const double* rkpt, int ntype, const int* natom, const double* rat,
+                               int mxdatm, const double* adot, const int* nqnl, const double* delqnl,
+                               const double* vkb, int mxdlqp, const int* nkb, int nanl, double* xnlkb,
+                               void* anlga, long long ldanl) {
+  if (int s = check_ctx(c)) return s;
+  cudaSetDevice(c->device);
+  return ctx_proj_nl_kb(c, rkpt, ntype, natom, rat, mxdatm, adot, nqnl, delqnl, vkb, mxdlqp, nkb, nanl, xnlkb, anlga,
+                        ldanl);
+}
+
 int cpw_b200_hk_psi_device(cpw_b200_ctx* c, int neig, const void* psi, long long ldpsi, void* hpsi, long long ldh,
                            void* stream) {
   if (int s = check_ctx(c)) return s;

@@ -143,6 +143,9 @@ int ctx_set_basis(cpw_b200_ctx* c, int mtxd, const int* isort, const int* kgv, i
                   const int* kmscr);
 int ctx_set_potential(cpw_b200_ctx* c, const double* vscr, long long nscr);
 int ctx_set_projectors(cpw_b200_ctx* c, int nanl, const double* anlga, int ld, const double* xnlkb, bool on_device);
+int ctx_proj_nl_kb(cpw_b200_ctx* c, const double* rkpt, int ntype, const int* natom, const double* rat, int mxdatm,
+                   const double* adot, const int* nqnl, const double* delqnl, const double* vkb, int mxdlqp,
+                   const int* nkb, int nanl, double* xnlkb_out, void* anlga_out, long long ld_out);
 int ctx_hkpsi_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh,
                      cudaStream_t st, bool with_kinetic, bool with_nl);
 }  // namespace cpwb

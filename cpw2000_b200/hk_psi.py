@@ -14,7 +14,7 @@ import ctypes as C
 
 import numpy as np
 
-from . import _lib
+from . import _lib, pseudo
 from ._lib import check, dptr, iptr, zptr
 
 FP64 = 0
@@ -150,6 +150,47 @@ class Context:
         check(self._L.cpw_b200_set_projectors(self.handle, nanl, zptr(a), int(a.shape[0]),
                                               dptr(x)))
         self.nanl = nanl
+
+    def proj_nl_kb(self, rkpt, species, vkb, nkb, adot, delq: float = 0.01, nq: int = 4000, anlga_out=None):
+        """Build the KB projectors of the current k-point on the device and install them
+        (cpw_b200_proj_nl_kb_device, the device form of Src/omp/proj_nl_kb_c16.f90).
+
+        species: list of pseudo.Species (natom, rat); vkb[ntype, 4, nq+3] and nkb[ntype, 4] as
+        returned by pseudo.kb_tables; adot the real-space metric. The tables are passed in the
+        reference layouts vkb(-2:nq, 0:3, -1:1, ntype) and nkb(0:3, -1:1, ntype) (spin-orbit
+        channel 0). anlga_out: optional complex128 CUDA tensor (mtxd, nanl) column-major that
+        receives a copy. Returns xnlkb (numpy)."""
+        ntype = len(species)
+        natom = np.array([sp.natom for sp in species], dtype=np.int32)
+        mxdatm = max(1, int(natom.max()) if ntype else 1)
+        rat = np.zeros((3, mxdatm, max(ntype, 1)), order="F")
+        for t, sp in enumerate(species):
+            if sp.natom:
+                rat[:, :sp.natom, t] = np.asarray(sp.rat, dtype=np.float64).T
+        vkb = np.asarray(vkb, dtype=np.float64)
+        vref = np.zeros((nq + 3, 4, 3, max(ntype, 1)), order="F")
+        nref = np.zeros((4, 3, max(ntype, 1)), dtype=np.int32, order="F")
+        for t in range(ntype):
+            for l in range(4):
+                vref[:, l, 1, t] = vkb[t, l, :nq + 3]
+                nref[l, 1, t] = int(nkb[t, l])
+        nanl = pseudo.nanl_of(species, np.asarray(nkb))
+        xnl = np.zeros(max(nanl, 1))
+        rk = np.ascontiguousarray(rkpt, dtype=np.float64)
+        ad = np.asfortranarray(adot, dtype=np.float64)
+        nqa = np.full(max(ntype, 1), nq, dtype=np.int32)
+        dqa = np.full(max(ntype, 1), delq, dtype=np.float64)
+        out_ptr, ld = None, 0
+        if anlga_out is not None:
+            if anlga_out.stride(0) != 1:
+                raise ValueError("anlga_out must be column-major")
+            out_ptr = C.c_void_p(anlga_out.data_ptr())
+            ld = int(anlga_out.stride(1)) if anlga_out.shape[1] > 1 else self.mtxd
+        check(self._L.cpw_b200_proj_nl_kb_device(self.handle, dptr(rk), ntype, iptr(natom), dptr(rat), mxdatm,
+                                                 dptr(ad), iptr(nqa), dptr(dqa), dptr(vref), nq, iptr(nref), nanl,
+                                                 dptr(xnl), out_ptr, ld))
+        self.nanl = nanl
+        return xnl[:nanl]
 
     def setup(self, inputs: dict):
         """Upload one k-point from a dict as returned by configs.kpoint_inputs."""

@@ -91,6 +91,21 @@ int cpw_b200_set_potential(cpw_b200_ctx* ctx, const double* vscr, long long mxds
 int cpw_b200_set_projectors(cpw_b200_ctx* ctx, int nanl, const double* anlga, int mxddim, const double* xnlkb);
 /* Same with device pointers (anlga complex128, leading dimension ld). */
 int cpw_b200_set_projectors_device(cpw_b200_ctx* ctx, int nanl, const void* anlga, int ld, const void* xnlkb);
+/* KB projectors of the context's k-point computed on the device: replaces
+ * Src/omp/proj_nl_kb_c16.f90:23-275 (same arguments: rkpt(3) lattice
+ * coordinates of k, natom(ntype), rat(3, mxdatm, ntype) lattice coordinates,
+ * adot(3,3) metric, nqnl(ntype), delqnl(ntype), vkb(-2:mxdlqp, 0:3, -1:1, ntype)
+ * and nkb(0:3, -1:1, ntype) as in the reference; host arrays) followed by
+ * cpw_b200_set_projectors, without the host loop and the mtxd x nanl upload.
+ * The basis is the one given to cpw_b200_set_kpoint. nanl must equal
+ * sum_type natom * sum_{l: nkb(l,0,type) != 0} (2l+1) (the reference's check).
+ * xnlkb (host, nanl) may be NULL; anlga (device, complex128, leading dimension
+ * ldanl >= mtxd) may be NULL, else it receives a copy of the projectors.
+ * Synchronous. */
+int cpw_b200_proj_nl_kb_device(cpw_b200_ctx* ctx, const double* rkpt, int ntype, const int* natom,
+                               const double* rat, int mxdatm, const double* adot, const int* nqnl,
+                               const double* delqnl, const double* vkb, int mxdlqp, const int* nkb, int nanl,
+                               double* xnlkb, void* anlga, long long ldanl);
 
 /* hpsi = H psi for neig device-resident complex128 columns (ld >= mtxd), on
  * `stream` (cudaStream_t; NULL = the context stream). Asynchronous.
