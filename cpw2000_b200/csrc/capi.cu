@@ -402,6 +402,35 @@ int cpw_b200_proj_nl_kb_device(cpw_b200_ctx* c, const double* rkpt, int ntype, c
                         ldanl);
 }
 
+int cpw_b200_pot_local(cpw_b200_ctx* c, double* vscr, double* vmax, double* vmin, double* cmax, const double* veff,
+                       int* kmscr, int idshift, int ng, const int* kgv, const double* phase, const double* conj, int ns,
+                       const int* inds, int mxdscr, int mxdgve, int mxdnst, int install) {
+  if (int s = check_ctx(c)) return s;
+  // the checks of pot_local.f90:104-120 and the bounds it assumes
+  if (ng < 0 || ng > mxdgve) return fail(kBadArg, "pot_local: ng out of range of mxdgve");
+  if (ns < 0 || ns > mxdnst) return fail(kBadArg, "pot_local: ns out of range of mxdnst");
+  if (idshift < 0) return fail(kBadArg, "pot_local: idshift < 0");
+  for (int i = 0; i < ng; ++i)
+    if (inds[i] < 1 || inds[i] > ns) return fail(kBadArg, "pot_local: inds out of range 1..ns");
+  int n[3];
+  size_fft(kmscr, n);
+  const long long mxdwrk =
+      4LL * std::max((long long)n[0] * n[1], std::max((long long)n[0] * n[2], (long long)n[1] * n[2]));
+  if (mxdwrk > mxdscr) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "pot_local: mxdwrk = %lld is greater than mxdscr = %d", mxdwrk, mxdscr);
+    return fail(kBadArg, buf);
+  }
+  const int id = n[0] + idshift;
+  if (vscr && (long long)id * n[1] * n[2] > mxdscr) return fail(kBadArg, "pot_local: vscr (mxdscr) smaller than id*n2*n3");
+  kmscr[3] = n[0];
+  kmscr[4] = n[1];
+  kmscr[5] = n[2];
+  kmscr[6] = id;
+  cudaSetDevice(c->device);
+  return ctx_pot_local(c, n[0], n[1], n[2], id, ng, kgv, veff, phase, conj, inds, vscr, vmax, vmin, cmax, install != 0);
+}
+
 int cpw_b200_hk_psi_device(cpw_b200_ctx* c, int neig, const void* psi, long long ldpsi, void* hpsi, long long ldh,
                            void* stream) {
   if (int s = check_ctx(c)) return s;

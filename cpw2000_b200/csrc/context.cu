@@ -60,7 +60,7 @@ void DevBuf::release() {
 }
 
 // Split n = r1*r2 with both factors supported radices, as balanced as possible.
-static bool factor(int n, FftDim& d) {
+bool factor(int n, FftDim& d) {
   int best = -1;
   for (int r1 = 1; r1 <= 16; ++r1) {
     if (n % r1) continue;
@@ -76,7 +76,7 @@ static bool factor(int n, FftDim& d) {
 }
 
 // W_n^k = exp(-2 pi i k / n), k = 0..n-1, in long double then rounded.
-static void twiddles(int n, std::vector<double>& out) {
+void twiddles(int n, std::vector<double>& out) {
   out.resize(2 * (size_t)n);
   const long double tp = 6.283185307179586476925286766559005768L;
   for (int k = 0; k < n; ++k) {

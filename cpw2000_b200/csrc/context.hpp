@@ -62,6 +62,12 @@ int plan_for_box(cpw_b200_ctx* c, const int kd[3], const int* kmscr, LocalPlan* 
 void plane_lists(const LocalPlan& p, int mtxd, const int* g, std::vector<int>& start, std::vector<int>& idx,
                  std::vector<int>& pos);
 int upload(DevBuf& b, const void* h, size_t bytes);
+// n = r1*r2 with both factors supported radices (false if none); W_n^k = e^{-2 pi i k/n}
+bool factor(int n, FftDim& d);
+void twiddles(int n, std::vector<double>& out);
+int ctx_pot_local(cpw_b200_ctx* c, int n1, int n2, int n3, int id, int ng, const int* kgv, const double* veff,
+                  const double* phase, const double* conj, const int* inds, double* vscr, double* vmax,
+                  double* vmin, double* cmax, bool install);
 // per-call scratch of the tensor-core projector products and their sticky error flag
 struct TcScratch {
   DevBuf b1, part, b2, err;

@@ -14,7 +14,7 @@ import ctypes as C
 
 import numpy as np
 
-from . import _lib, pseudo
+from . import _lib, crystal, pseudo
 from ._lib import check, dptr, iptr, zptr
 
 FP64 = 0
@@ -191,6 +191,35 @@ class Context:
                                                  dptr(xnl), out_ptr, ld))
         self.nanl = nanl
         return xnl[:nanl]
+
+    def pot_local(self, veff, kgv, inds, phase=None, conj=None, kmscr=(0, 0, 0), idshift: int = 0,
+                  install: bool = True, want_vscr: bool = True):
+        """Screened potential on the mesh from its values per star (cpw_b200_pot_local, the
+        device form of Src/cpw_lib/pot_local.f90). veff (ns,) complex; kgv (3, ng) int;
+        inds (ng,) 1-based stars; phase (ng,) complex (default 1); conj (ng,) +-1 (default +1);
+        kmscr(1:3) the extent of G on the mesh. install: also make it this context's potential.
+        Returns dict(vscr, vmax, vmin, cmax, kmscr)."""
+        veff = np.ascontiguousarray(veff, dtype=np.complex128)
+        kgv = np.asfortranarray(kgv, dtype=np.int32)
+        ng = int(kgv.shape[1])
+        inds = np.ascontiguousarray(inds, dtype=np.int32)
+        phase = np.ones(ng, np.complex128) if phase is None else np.ascontiguousarray(phase, dtype=np.complex128)
+        conj = np.ones(ng) if conj is None else np.ascontiguousarray(conj, dtype=np.float64)
+        km = np.zeros(7, dtype=np.int32)
+        km[:3] = np.asarray(kmscr, dtype=np.int32)[:3]
+        ns = int(veff.size)
+        # the mesh is size_fft(kmscr); the library checks it and sets kmscr(4:7)
+        n1, n2, n3 = crystal.size_fft(km[:3])
+        mxdscr = max((n1 + idshift) * n2 * n3, 4 * max(n1 * n2, n1 * n3, n2 * n3))
+        vscr = np.zeros(mxdscr) if want_vscr else None
+        vmax, vmin, cmax = C.c_double(), C.c_double(), C.c_double()
+        check(self._L.cpw_b200_pot_local(self.handle, dptr(vscr) if want_vscr else None, C.byref(vmax),
+                                         C.byref(vmin), C.byref(cmax), zptr(veff), iptr(km), int(idshift), ng,
+                                         iptr(kgv), zptr(phase), dptr(conj), ns, iptr(inds), mxdscr, ng,
+                                         max(ns, 1), 1 if install else 0))
+        n1, n2, n3, ident = (int(x) for x in km[3:7])
+        return dict(vscr=vscr[:ident * n2 * n3] if want_vscr else None, vmax=vmax.value, vmin=vmin.value,
+                    cmax=cmax.value, kmscr=km)
 
     def setup(self, inputs: dict):
         """Upload one k-point from a dict as returned by configs.kpoint_inputs."""

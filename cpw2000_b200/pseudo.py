@@ -224,6 +224,29 @@ def local_potential_box(species, adot, box, idpad: int = 0):
     return box_arr.reshape(-1), veffr1
 
 
+def local_potential_coefficients(species, adot, box):
+    """V(G) of local_potential_box as a list of G vectors: (kgv (3, ng) int32 signed
+    reciprocal-lattice coordinates, V (ng,) complex128), every G of the box except the Nyquist
+    planes. With one star per G (inds = 1..ng, phase 1, conj +1) these are the veff, kgv,
+    phase, conj and inds arguments of pot_local (Src/cpw_lib/pot_local.f90) that reproduce
+    local_potential_box's vscr."""
+    n1, n2, n3 = box
+    vcell, bdot = adot_to_bdot(adot)
+    m = [np.fft.fftfreq(n, 1.0 / n).astype(np.int64) for n in (n1, n2, n3)]
+    m1, m2, m3 = np.meshgrid(*m, indexing="ij")
+    keep = np.ones(m1.shape, dtype=bool)
+    for mi, n in ((m1, n1), (m2, n2), (m3, n3)):
+        if n % 2 == 0:
+            keep &= mi != -(n // 2)
+    g = np.stack([m1[keep], m2[keep], m3[keep]]).astype(np.float64)
+    g2 = np.einsum("in,ij,jn->n", g, bdot, g)
+    vg = np.zeros(g.shape[1], dtype=np.complex128)
+    for sp in species:
+        ff = -sp.v0 * (2 * PI * sp.sigma ** 2) ** 1.5 * np.exp(-0.5 * g2 * sp.sigma ** 2) / vcell
+        vg += ff * np.exp(-2j * PI * (np.asarray(sp.rat) @ g)).sum(axis=0)
+    return np.asfortranarray(g.astype(np.int32)), vg
+
+
 def local_form_factors_box(species, adot, box):
     """Form factors v_t(G) of every species on the box, FFT order, shape (ntype, n3, n2, n1).
 

@@ -107,6 +107,21 @@ int cpw_b200_proj_nl_kb_device(cpw_b200_ctx* ctx, const double* rkpt, int ntype,
                                const double* delqnl, const double* vkb, int mxdlqp, const int* nkb, int nanl,
                                double* xnlkb, void* anlga, long long ldanl);
 
+/* Screened local potential on the FFT mesh, computed on the device: replaces
+ * Src/cpw_lib/pot_local.f90:1-190 (same arguments and array layouts, host
+ * arrays: veff(mxdnst) complex(8) per star, kmscr(7) in/out (kmscr(4:7) set to
+ * n1, n2, n3, id = n1 + idshift), kgv(3, mxdgve), phase(mxdgve) complex(8),
+ * conj(mxdgve), inds(mxdgve) 1-based stars; ipr dropped). vscr(id*n2*n3)
+ * (host, may be NULL) receives the real potential; vmax/vmin its extrema and
+ * cmax the largest imaginary part (each may be NULL). Fails like the
+ * reference's stop when cmax > 1e-6. install != 0 also makes it the context's
+ * potential without a host round trip (the context's k-point box must be the
+ * same mesh). G vectors outside the mesh wrap modulo the mesh. Synchronous. */
+int cpw_b200_pot_local(cpw_b200_ctx* ctx, double* vscr, double* vmax, double* vmin, double* cmax,
+                       const double* veff, int* kmscr, int idshift, int ng, const int* kgv,
+                       const double* phase, const double* conj, int ns, const int* inds, int mxdscr,
+                       int mxdgve, int mxdnst, int install);
+
 /* hpsi = H psi for neig device-resident complex128 columns (ld >= mtxd), on
  * `stream` (cudaStream_t; NULL = the context stream). Asynchronous.
  * Same operator as hk_psi_c16.f90:176-231. */

@@ -182,3 +182,18 @@ def test_golden_hkpsi_fixture():
     hp = O.hk_psi_c16(d["mtxd"], z["psi"].shape[1], z["psi"], d["ekpg"], d["isort"], d["vscr"], d["kmscr"],
                       d["kgv"], d["anlga"], d["xnlkb"])
     assert np.abs(hp - z["hpsi"]).max() < 1e-12 * np.abs(z["hpsi"]).max()
+
+
+def test_potential_coefficients_reproduce_host_vscr():
+    # the star arguments the pot_local tests give the device reproduce the host potential
+    from cpw2000_b200 import configs as CF, pseudo as PS
+    w = CF.WORKLOADS["si2"]()
+    want, _ = PS.local_potential_box(w.species, w.adot, w.box, 2)
+    kgv, vg = PS.local_potential_coefficients(w.species, w.adot, w.box)
+    n1, n2, n3 = w.box
+    box = np.zeros((n1, n2, n3), complex)
+    box[kgv[0] % n1, kgv[1] % n2, kgv[2] % n3] = vg
+    vr = np.fft.ifftn(box) * box.size
+    got = np.zeros((n3, n2, n1 + 2))
+    got[:, :, :n1] = vr.real.transpose(2, 1, 0)
+    assert np.abs(got.ravel() - want).max() <= 1e-13 * np.abs(want).max()
