@@ -37,6 +37,12 @@ SIGNATURES = {
     "cpw_b200_set_projectors_device": (I, [P, I, P, I, P]),
     "cpw_b200_proj_nl_kb_device": (I, [P, DP, I, IP, DP, I, DP, IP, DP, DP, I, IP, I, DP, P, LL]),
     "cpw_b200_pot_local": (I, [P, DP, DP, DP, DP, DP, IP, I, I, IP, DP, DP, I, IP, I, I, I, I]),
+    "cpw_b200_set_potential_spin": (I, [P, DP, LL, I]),
+    "cpw_b200_set_projectors_spin": (I, [P, I, DP, LL, DP]),
+    "cpw_b200_hk_psi_spin_device": (I, [P, I, P, LL, P, LL, P]),
+    "cpw_b200_hk_psi_spin_c16": (I, [IP, IP, DP, DP, IP, IP, IP, DP, IP, DP, IP, IP, DP, DP, IP, IP, IP, IP, IP, IP,
+                                     IP]),
+    "hk_psi_spin_c16_": (None, [IP, IP, DP, DP, IP, IP, IP, DP, IP, DP, IP, IP, DP, DP, IP, IP, IP, IP, IP, IP, IP]),
     "cpw_b200_hk_psi_device": (I, [P, I, P, LL, P, LL, P]),
     "cpw_b200_hk_psi_loc_device": (I, [P, I, P, LL, P, LL, P]),
     "cpw_b200_hk_psi_c16": (I, [IP, IP, DP, DP, IP, IP, IP, DP, IP, DP, IP, DP, DP, IP, IP, IP, IP, IP, IP]),

@@ -431,6 +431,26 @@ int cpw_b200_pot_local(cpw_b200_ctx* c, double* vscr, double* vmax, double* vmin
   return ctx_pot_local(c, n[0], n[1], n[2], id, ng, kgv, veff, phase, conj, inds, vscr, vmax, vmin, cmax, install != 0);
 }
 
+int cpw_b200_set_potential_spin(cpw_b200_ctx* c, const double* vscr_sp, long long mxdscr, int nsp) {
+  if (int s = check_ctx(c)) return s;
+  cudaSetDevice(c->device);
+  return ctx_set_potential_spin(c, vscr_sp, mxdscr, nsp);
+}
+
+int cpw_b200_set_projectors_spin(cpw_b200_ctx* c, int nanlsp, const double* anlsp, long long ld, const double* xnlkbsp) {
+  if (int s = check_ctx(c)) return s;
+  cudaSetDevice(c->device);
+  return ctx_set_projectors_spin(c, nanlsp, anlsp, ld, xnlkbsp);
+}
+
+int cpw_b200_hk_psi_spin_device(cpw_b200_ctx* c, int neig, const void* psi_sp, long long ldpsi, void* hpsi_sp,
+                                long long ldh, void* stream) {
+  if (int s = check_ctx(c)) return s;
+  cudaSetDevice(c->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  return ctx_hkpsi_spin_device(c, neig, psi_sp, ldpsi, hpsi_sp, ldh, st);
+}
+
 int cpw_b200_hk_psi_device(cpw_b200_ctx* c, int neig, const void* psi, long long ldpsi, void* hpsi, long long ldh,
                            void* stream) {
   if (int s = check_ctx(c)) return s;
@@ -518,6 +538,98 @@ void hk_psi_c16_(const int* mtxd, const int* neig, const double* psi, double* hp
   int s = cpw_b200_hk_psi_c16(mtxd, neig, psi, hpsi, lnewanl, ng, kgv, ekpg, isort, vscr, kmscr, anlga, xnlkb, nanl,
                               mxddim, mxdbnd, mxdanl, mxdgve, mxdscr);
   if (s) stop_like_fortran("hk_psi_c16");
+}
+
+namespace {
+// the spinor drop-in keeps its own context and host shadows of its k-point and potential
+struct SpinDropin {
+  cpw_b200_ctx* c = nullptr;
+  std::vector<int> isort, kgv, kmscr;
+  std::vector<double> ekpg, vscr;
+  int nanl = -1;
+};
+SpinDropin g_spin;
+std::mutex g_spin_mu;
+}  // namespace
+
+int cpw_b200_hk_psi_spin_c16(const int* mtxd, const int* neig, const double* psi_sp, double* hpsi_sp, int* lnewanl,
+                             const int* ng, const int* kgv, const double* ekpg, const int* isort,
+                             const double* vscr_sp, const int* kmscr, const int* nsp, const double* anlsp,
+                             const double* xnlkbsp, const int* nanlsp, const int* mxddim, const int* mxdbnd,
+                             const int* mxdasp, const int* mxdgve, const int* mxdscr, const int* mxdnsp) {
+  // argument checks of hk_psi_spin_c16.f90 and the array bounds it assumes
+  if (*ng > *mxdgve) return fail(kBadArg, "hk_psi_spin_c16: ng > mxdgve");
+  if (*nsp > *mxdnsp) return fail(kBadArg, "hk_psi_spin_c16: nsp is greater than mxdnsp");
+  if (*nsp != 1 && *nsp != 2 && *nsp != 4) return fail(kBadArg, "hk_psi_spin_c16: nsp is an incorrect value, should be 1,2,4");
+  if (*mtxd < 0 || *mtxd > *mxddim) return fail(kBadArg, "hk_psi_spin_c16: mtxd out of range of mxddim");
+  if (*neig < 0 || *neig > *mxdbnd) return fail(kBadArg, "hk_psi_spin_c16: neig out of range of mxdbnd");
+  if (*nanlsp < 0 || *nanlsp > *mxdasp) return fail(kBadArg, "hk_psi_spin_c16: nanlsp out of range of mxdasp");
+  {
+    int ns[3];
+    size_fft(kmscr, ns);
+    const long long mxdwrk =
+        4LL * std::max((long long)ns[0] * ns[1], std::max((long long)ns[0] * ns[2], (long long)ns[1] * ns[2]));
+    if (mxdwrk > *mxdscr) {
+      char buf[160];
+      snprintf(buf, sizeof buf, "hk_psi_spin_c16: mxdwrk = %lld is greater than mxdscr = %d", mxdwrk, *mxdscr);
+      return fail(kBadArg, buf);
+    }
+    if ((long long)kmscr[6] * kmscr[4] * kmscr[5] > *mxdscr)
+      return fail(kBadArg, "hk_psi_spin_c16: vscr_sp (mxdscr) smaller than id*n2*n3");
+  }
+  std::lock_guard<std::mutex> lk(g_spin_mu);
+  SpinDropin& d = g_spin;
+  int s;
+  if (!d.c) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if ((s = cpw_b200_create(&d.c, dev))) return s;
+  }
+  cpw_b200_ctx* c = d.c;
+  cudaSetDevice(c->device);
+  const int m = *mtxd, nb = *neig;
+  bool new_basis = !(d.isort.size() == (size_t)m && same(d.isort, isort, m) && same(d.ekpg, ekpg, m) &&
+                     same(d.kmscr, kmscr, 7) && same(d.kgv, kgv, 3 * (size_t)*ng));
+  if (new_basis) {
+    if ((s = ctx_set_basis(c, m, isort, kgv, *ng, ekpg, kmscr))) return s;
+    d.isort.assign(isort, isort + m);
+    d.ekpg.assign(ekpg, ekpg + m);
+    d.kmscr.assign(kmscr, kmscr + 7);
+    d.kgv.assign(kgv, kgv + 3 * (size_t)*ng);
+    d.vscr.clear();
+  }
+  const size_t nv = (size_t)*mxdscr * *nsp;
+  if (new_basis || c->nsp != *nsp || !same(d.vscr, vscr_sp, nv)) {
+    if ((s = ctx_set_potential_spin(c, vscr_sp, *mxdscr, *nsp))) return s;
+    d.vscr.assign(vscr_sp, vscr_sp + nv);
+  }
+  if (new_basis || *lnewanl || d.nanl != *nanlsp) {
+    if ((s = ctx_set_projectors_spin(c, *nanlsp, anlsp, 2LL * *mxddim, xnlkbsp))) return s;
+    d.nanl = *nanlsp;
+    *lnewanl = 0;
+  }
+  if (m == 0 || nb == 0) return kOk;
+  const size_t rows = 2 * (size_t)m;
+  const size_t bytes = rows * nb * 16;
+  if ((s = c->h_in.ensure(bytes)) || (s = c->h_out.ensure(bytes))) return s;
+  cudaError_t e = cudaMemcpy2DAsync(c->h_in.p, rows * 16, psi_sp, 2 * (size_t)*mxddim * 16, rows * 16, nb,
+                                    cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "hk_psi_spin_c16 H2D");
+  if ((s = ctx_hkpsi_spin_device(c, nb, c->h_in.p, (long long)rows, c->h_out.p, (long long)rows, c->stream))) return s;
+  e = cudaMemcpy2DAsync(hpsi_sp, 2 * (size_t)*mxddim * 16, c->h_out.p, rows * 16, rows * 16, nb,
+                        cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? kOk : cuda_fail(e, "hk_psi_spin_c16");
+}
+
+void hk_psi_spin_c16_(const int* mtxd, const int* neig, const double* psi_sp, double* hpsi_sp, int* lnewanl,
+                      const int* ng, const int* kgv, const double* ekpg, const int* isort, const double* vscr_sp,
+                      const int* kmscr, const int* nsp, const double* anlsp, const double* xnlkbsp,
+                      const int* nanlsp, const int* mxddim, const int* mxdbnd, const int* mxdasp, const int* mxdgve,
+                      const int* mxdscr, const int* mxdnsp) {
+  int s = cpw_b200_hk_psi_spin_c16(mtxd, neig, psi_sp, hpsi_sp, lnewanl, ng, kgv, ekpg, isort, vscr_sp, kmscr, nsp,
+                                   anlsp, xnlkbsp, nanlsp, mxddim, mxdbnd, mxdasp, mxdgve, mxdscr, mxdnsp);
+  if (s) stop_like_fortran("hk_psi_spin_c16");
 }
 
 int cpw_b200_ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, double epspsi, int* neig,

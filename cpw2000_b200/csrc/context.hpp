@@ -133,6 +133,14 @@ struct cpw_b200_ctx {
   long long tc_k1p = 0, tc_k2p = 0;     // K blocks (32 reals) of the projection and expansion operands
   bool tc_ready = false;
 
+  // two-component spinors (hk_psi_spin_c16): nsp potential combinations scaled by 1/N
+  // ([V] or [V1+V2, V1-V2] or [V1+V2, V1-V2, V3, -V4]), the spinor projectors (2 mtxd rows)
+  // and the component views of the basis (doubled plane-wave indices and kinetic diagonal)
+  int nsp = 0;
+  cpwb::DevBuf sp_v64[4], sp_v32[4];
+  int nanl_sp = 0;
+  cpwb::DevBuf anl_sp, anld_sp, sp_idx2, sp_ek2;
+
   cpwb::StageTimer timer;
 
   // slab for the band chunk and staging for host-array entry points
@@ -149,6 +157,10 @@ int ctx_set_basis(cpw_b200_ctx* c, int mtxd, const int* isort, const int* kgv, i
                   const int* kmscr);
 int ctx_set_potential(cpw_b200_ctx* c, const double* vscr, long long nscr);
 int ctx_set_projectors(cpw_b200_ctx* c, int nanl, const double* anlga, int ld, const double* xnlkb, bool on_device);
+int ctx_set_potential_spin(cpw_b200_ctx* c, const double* vscr_sp, long long mxdscr, int nsp);
+int ctx_set_projectors_spin(cpw_b200_ctx* c, int nanl, const double* anlsp, long long ld, const double* xnlkb);
+int ctx_hkpsi_spin_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh,
+                          cudaStream_t st);
 int ctx_proj_nl_kb(cpw_b200_ctx* c, const double* rkpt, int ntype, const int* natom, const double* rat, int mxdatm,
                    const double* adot, const int* nqnl, const double* delqnl, const double* vkb, int mxdlqp,
                    const int* nkb, int nanl, double* xnlkb_out, void* anlga_out, long long ld_out);

@@ -54,7 +54,7 @@ template cudaError_t launch_local<float>(CPWB_LAUNCH_ARGS(float));
 
 template <typename T>
 cudaError_t launch_inverse_xy(CPWB_INV_ARGS(T)) {
-  const bool cubic = p.n1 == p.n2 && p.n2 == p.n3 && p.tcol == 32 && p.cb == 32;
+  const bool cubic = p.n1 == p.n2 && p.n2 == p.n3 && p.tcol == 32;   // kernel A does not depend on the z tile
   if (cubic && is_split(p.dx, 8, 12))
     return kern::launch_inv_impl<T, 8, 12, 8, 12, 32>(p, nbc, band0, psi, ldpsi, plane_start, pw_idx, pw_pos, twx,
                                                      twy, W, st);

@@ -221,6 +221,30 @@ class Context:
         return dict(vscr=vscr[:ident * n2 * n3] if want_vscr else None, vmax=vmax.value, vmin=vmin.value,
                     cmax=cmax.value, kmscr=km)
 
+    def set_potential_spin(self, vscr_sp, nsp: int):
+        """vscr_sp: (mxdscr, nsp) real, columns (1, sigma_z, sigma_x, sigma_y) of the box."""
+        v = np.asfortranarray(vscr_sp, dtype=np.float64)
+        check(self._L.cpw_b200_set_potential_spin(self.handle, dptr(v), int(v.shape[0]), int(nsp)))
+
+    def set_projectors_spin(self, anlsp, xnlkbsp):
+        """Spinor KB projectors anlsp (2*mtxd, nanlsp) complex128 and xnlkbsp (nanlsp,)."""
+        a = np.asfortranarray(anlsp, dtype=np.complex128)
+        x = np.ascontiguousarray(xnlkbsp, dtype=np.float64)
+        if x.size == 0:
+            a = np.zeros((max(2 * self.mtxd, 1), 1), np.complex128, order="F")
+            x = np.zeros(1)
+            n = 0
+        else:
+            n = int(x.size)
+        check(self._L.cpw_b200_set_projectors_spin(self.handle, n, zptr(a), int(a.shape[0]), dptr(x)))
+
+    def hk_psi_spin(self, psi_sp, hpsi_sp):
+        """hpsi_sp = H psi_sp for column-major complex128 CUDA tensors (2*mtxd, nb), rows
+        interleaved (up, down) per plane wave, on torch's current stream."""
+        check(self._L.cpw_b200_hk_psi_spin_device(self.handle, int(psi_sp.shape[1]), C.c_void_p(psi_sp.data_ptr()),
+                                                  self._ld(psi_sp), C.c_void_p(hpsi_sp.data_ptr()),
+                                                  self._ld(hpsi_sp), C.c_void_p(torch_stream_handle(psi_sp.device))))
+
     def setup(self, inputs: dict):
         """Upload one k-point from a dict as returned by configs.kpoint_inputs."""
         self.set_kpoint(inputs["mtxd"], inputs["isort"], inputs["kgv"], inputs["ekpg"], inputs["kmscr"])

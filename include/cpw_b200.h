@@ -10,6 +10,7 @@
  *     reference's leading dimensions, 1-based isort into kgv(3, mxdgve):
  *       cpw_b200_hk_psi_c16  / hk_psi_c16_    replaces Src/hk_psi/reference/hk_psi_c16.f90:28-32
  *       cpw_b200_hk_psi_nl_c16 / hk_psi_nl_c16_ replaces Src/cpw_lib/hk_psi_nl_c16.f90:23-24
+ *       cpw_b200_hk_psi_spin_c16 / hk_psi_spin_c16_ replaces Src/hk_psi/reference/hk_psi_spin_c16.f90:1-316
  *       cpw_b200_ditsp_c16   / ditsp_c16_     replaces Src/ditsp/ditsp_c16.f90:20-27
  *     The cpw_b200_* forms return a status (0 = success) and never stop the
  *     program; the trailing-underscore forms are link-time substitutes for the
@@ -122,6 +123,18 @@ int cpw_b200_pot_local(cpw_b200_ctx* ctx, double* vscr, double* vmax, double* vm
                        const double* phase, const double* conj, int ns, const int* inds, int mxdscr,
                        int mxdgve, int mxdnst, int install);
 
+/* Spinor form on a context (the k-point from cpw_b200_set_kpoint): the nsp
+ * potential columns vscr_sp(mxdscr, nsp) (host), the spinor projectors
+ * anlsp(ld >= 2*mtxd, nanlsp) and xnlkbsp (host), then hpsi_sp = H psi_sp for
+ * neig device-resident spinors (complex128, ld >= 2*mtxd, rows interleaved up,
+ * down) on `stream` (NULL = the context stream). MIXED contexts run the local
+ * part in FP32; the projector products are FP64 in every form. */
+int cpw_b200_set_potential_spin(cpw_b200_ctx* ctx, const double* vscr_sp, long long mxdscr, int nsp);
+int cpw_b200_set_projectors_spin(cpw_b200_ctx* ctx, int nanlsp, const double* anlsp, long long ld,
+                                 const double* xnlkbsp);
+int cpw_b200_hk_psi_spin_device(cpw_b200_ctx* ctx, int neig, const void* psi_sp, long long ldpsi, void* hpsi_sp,
+                                long long ldh, void* stream);
+
 /* hpsi = H psi for neig device-resident complex128 columns (ld >= mtxd), on
  * `stream` (cudaStream_t; NULL = the context stream). Asynchronous.
  * Same operator as hk_psi_c16.f90:176-231. */
@@ -172,6 +185,24 @@ void hk_psi_c16_(const int* mtxd, const int* neig, const double* psi, double* hp
                  const int* kgv, const double* ekpg, const int* isort, const double* vscr, const int* kmscr,
                  const double* anlga, const double* xnlkb, const int* nanl, const int* mxddim, const int* mxdbnd,
                  const int* mxdanl, const int* mxdgve, const int* mxdscr);
+
+/* Src/hk_psi/reference/hk_psi_spin_c16.f90: H|psi> of two-component spinors,
+ * psi_sp/hpsi_sp complex(8)(2*mxddim, mxdbnd) with the up component of plane
+ * wave i at row 2i-1 and the down component at row 2i (1-based), vscr_sp
+ * real(8)(mxdscr, mxdnsp) with nsp = 1, 2 or 4 columns (1, sigma_z, sigma_x,
+ * sigma_y), anlsp complex(8)(2*mxddim, mxdasp) spinor KB projectors. The
+ * k-point arrays and vscr_sp are compared with the previous call's; anlsp is
+ * re-uploaded when lnewanl != 0 (then cleared), nanlsp or the basis changed. */
+int cpw_b200_hk_psi_spin_c16(const int* mtxd, const int* neig, const double* psi_sp, double* hpsi_sp,
+                             int* lnewanl, const int* ng, const int* kgv, const double* ekpg, const int* isort,
+                             const double* vscr_sp, const int* kmscr, const int* nsp, const double* anlsp,
+                             const double* xnlkbsp, const int* nanlsp, const int* mxddim, const int* mxdbnd,
+                             const int* mxdasp, const int* mxdgve, const int* mxdscr, const int* mxdnsp);
+void hk_psi_spin_c16_(const int* mtxd, const int* neig, const double* psi_sp, double* hpsi_sp, int* lnewanl,
+                      const int* ng, const int* kgv, const double* ekpg, const int* isort, const double* vscr_sp,
+                      const int* kmscr, const int* nsp, const double* anlsp, const double* xnlkbsp,
+                      const int* nanlsp, const int* mxddim, const int* mxdbnd, const int* mxdasp,
+                      const int* mxdgve, const int* mxdscr, const int* mxdnsp);
 
 /* Src/cpw_lib/hk_psi_nl_c16.f90:23-24: hpsi = [hpsi if ladd] + anlga xnlkb anlga^H psi. */
 int cpw_b200_hk_psi_nl_c16(const int* mtxd, const int* neig, const double* psi, double* hpsi, const double* anlga,

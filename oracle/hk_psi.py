@@ -2,6 +2,7 @@
 
 hk_psi_c16     -- Src/hk_psi/reference/hk_psi_c16.f90:28-241
 hk_psi_nl_c16  -- Src/cpw_lib/hk_psi_nl_c16.f90:23-104
+hk_psi_spin_c16 -- Src/hk_psi/reference/hk_psi_spin_c16.f90:1-316 (two-component spinors)
 dense_h        -- explicit matrix of the same operator (ground truth)
 """
 from __future__ import annotations
@@ -71,6 +72,47 @@ def hk_psi_c16(mtxd, neig, psi, ekpg, isort, vscr, kmscr, kgv, anlga, xnlkb):
         cfft_wf_c16(chd, ident, n1, n2, n3, kd1, kd2, kd3, 1)
         hpsi[:, n] = chd[ip] + ek * psi[:mtxd, n]
     hk_psi_nl_c16(psi[:mtxd, :neig], hpsi, anlga[:mtxd], xnlkb, ladd=True)
+    return hpsi
+
+
+def hk_psi_spin_c16(mtxd, neig, psi_sp, ekpg, isort, vscr_sp, kmscr, kgv, nsp, anlsp, xnlkbsp):
+    """H|psi> of spinors, Src/hk_psi/reference/hk_psi_spin_c16.f90.
+
+    psi_sp: (>= 2 mtxd, >= neig) complex128 with the up component of plane wave i at row 2i
+    and the down component at 2i+1 (0-based). vscr_sp: (>= id n2 n3, nsp) real, the columns
+    (1, sigma_z, sigma_x, sigma_y). Per spinor: both components to the box, backward pruned
+    FFT, the local potential (nsp 1: V on both; 2: V1+V2 on up, V1-V2 on down; 4: the 2x2
+    matrix [[V1+V2, V3-iV4], [V3+iV4, V1-V2]]), forward pruned FFT, gather, kinetic ekpg on
+    both components; then the KB term with 2 mtxd rows and the spinor projectors anlsp.
+    """
+    if nsp not in (1, 2, 4):
+        raise ValueError("hk_psi_spin_c16: nsp should be 1, 2 or 4")
+    n1, n2, n3, ident = (int(v) for v in kmscr[3:7])
+    ntot = ident * n2 * n3
+    ip, (kd1, kd2, kd3) = ipoint_of(mtxd, isort, kgv, kmscr)
+    v = np.asarray(vscr_sp, dtype=np.float64)[:ntot]
+    ek = np.asarray(ekpg[:mtxd], dtype=np.float64)
+    hpsi = np.zeros((2 * mtxd, neig), dtype=np.complex128)
+    for n in range(neig):
+        cp = np.zeros(ntot, dtype=np.complex128)
+        cm = np.zeros(ntot, dtype=np.complex128)
+        cp[ip] = psi_sp[0:2 * mtxd:2, n]
+        cm[ip] = psi_sp[1:2 * mtxd:2, n]
+        cfft_wf_c16(cp, ident, n1, n2, n3, kd1, kd2, kd3, -1)
+        cfft_wf_c16(cm, ident, n1, n2, n3, kd1, kd2, kd3, -1)
+        if nsp == 1:
+            cp, cm = v[:, 0] * cp, v[:, 0] * cm
+        elif nsp == 2:
+            cp, cm = (v[:, 0] + v[:, 1]) * cp, (v[:, 0] - v[:, 1]) * cm
+        else:
+            tp = (v[:, 0] + v[:, 1]) * cp + (v[:, 2] - 1j * v[:, 3]) * cm
+            tm = (v[:, 0] - v[:, 1]) * cm + (v[:, 2] + 1j * v[:, 3]) * cp
+            cp, cm = tp, tm
+        cfft_wf_c16(cp, ident, n1, n2, n3, kd1, kd2, kd3, 1)
+        cfft_wf_c16(cm, ident, n1, n2, n3, kd1, kd2, kd3, 1)
+        hpsi[0::2, n] = cp[ip] + ek * psi_sp[0:2 * mtxd:2, n]
+        hpsi[1::2, n] = cm[ip] + ek * psi_sp[1:2 * mtxd:2, n]
+    hk_psi_nl_c16(psi_sp[:2 * mtxd, :neig], hpsi, anlsp[:2 * mtxd], xnlkbsp, ladd=True)
     return hpsi
 
 

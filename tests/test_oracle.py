@@ -197,3 +197,27 @@ def test_potential_coefficients_reproduce_host_vscr():
     got = np.zeros((n3, n2, n1 + 2))
     got[:, :, :n1] = vr.real.transpose(2, 1, 0)
     assert np.abs(got.ravel() - want).max() <= 1e-13 * np.abs(want).max()
+
+
+def test_spin_restatement_components_and_hermiticity():
+    # nsp = 1 acts on each component like hk_psi_c16; the nsp = 4 operator is Hermitian
+    w = configs.WORKLOADS["si2"]()
+    d = configs.kpoint_inputs(w, 0)
+    m, nb = d["mtxd"], 2
+    rng = np.random.default_rng(0)
+    psi = rng.standard_normal((2 * m, nb)) + 1j * rng.standard_normal((2 * m, nb))
+    none2, none = np.zeros((2 * m, 0), complex), np.zeros((m, 0), complex)
+    h = O.hk_psi_spin_c16(m, nb, psi, d["ekpg"], d["isort"], d["vscr"][:, None], d["kmscr"], d["kgv"], 1, none2,
+                          np.zeros(0))
+    for c in range(2):
+        hc = O.hk_psi_c16(m, nb, np.ascontiguousarray(psi[c::2]), d["ekpg"], d["isort"], d["vscr"], d["kmscr"],
+                          d["kgv"], none, np.zeros(0))
+        assert np.abs(h[c::2] - hc).max() <= 1e-12 * np.abs(hc).max()
+    v4 = np.zeros((d["vscr"].size, 4))
+    v4[:, 0] = d["vscr"]
+    v4[:, 1:] = 0.3 * rng.standard_normal((d["vscr"].size, 3))
+    a, b = psi[:, :1], psi[:, 1:]
+    ha = O.hk_psi_spin_c16(m, 1, a, d["ekpg"], d["isort"], v4, d["kmscr"], d["kgv"], 4, none2, np.zeros(0))
+    hb = O.hk_psi_spin_c16(m, 1, b, d["ekpg"], d["isort"], v4, d["kmscr"], d["kgv"], 4, none2, np.zeros(0))
+    x, y = (b.conj() * ha).sum(), (hb.conj() * a).sum()
+    assert abs(x - y) <= 1e-12 * abs(x)
