@@ -431,6 +431,22 @@ int cpw_b200_pot_local(cpw_b200_ctx* c, double* vscr, double* vmax, double* vmin
   return ctx_pot_local(c, n[0], n[1], n[2], id, ng, kgv, veff, phase, conj, inds, vscr, vmax, vmin, cmax, install != 0);
 }
 
+int cpw_b200_hk_psi_kin_device(cpw_b200_ctx* c, int neig, const void* psi, long long ldpsi, void* hpsi, long long ldh,
+                               int ladd, int nspin, void* stream) {
+  if (int s = check_ctx(c)) return s;
+  cudaSetDevice(c->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  return ctx_hkpsi_kin_device(c, neig, psi, ldpsi, hpsi, ldh, ladd != 0, nspin, st);
+}
+
+int cpw_b200_hk_psi_loc_c16_device(cpw_b200_ctx* c, int neig, const void* psi, long long ldpsi, void* hpsi,
+                                   long long ldh, int ladd, int nspin, void* stream) {
+  if (int s = check_ctx(c)) return s;
+  cudaSetDevice(c->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  return ctx_hkpsi_loc_general(c, neig, psi, ldpsi, hpsi, ldh, ladd != 0, nspin, st);
+}
+
 int cpw_b200_set_potential_spin(cpw_b200_ctx* c, const double* vscr_sp, long long mxdscr, int nsp) {
   if (int s = check_ctx(c)) return s;
   cudaSetDevice(c->device);

@@ -159,6 +159,10 @@ int ctx_set_potential(cpw_b200_ctx* c, const double* vscr, long long nscr);
 int ctx_set_projectors(cpw_b200_ctx* c, int nanl, const double* anlga, int ld, const double* xnlkb, bool on_device);
 int ctx_set_potential_spin(cpw_b200_ctx* c, const double* vscr_sp, long long mxdscr, int nsp);
 int ctx_set_projectors_spin(cpw_b200_ctx* c, int nanl, const double* anlsp, long long ld, const double* xnlkb);
+int ctx_hkpsi_kin_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh,
+                         bool ladd, int nspin, cudaStream_t st);
+int ctx_hkpsi_loc_general(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh,
+                          bool ladd, int nspin, cudaStream_t st);
 int ctx_hkpsi_spin_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh,
                           cudaStream_t st);
 int ctx_proj_nl_kb(cpw_b200_ctx* c, const double* rkpt, int ntype, const int* natom, const double* rat, int mxdatm,

@@ -524,6 +524,11 @@ k_fwd_xy(LocalPlan p, int band0, const C2<double>* __restrict__ psi, long long l
       out.x += ek * s.x;
       out.y += ek * s.y;
     }
+    if (p.accum) {
+      const C2<double> h0 = hp[i];
+      out.x += h0.x;
+      out.y += h0.y;
+    }
     hp[i] = out;
   }
 }

@@ -55,6 +55,7 @@ struct LocalPlan {
   int tcol;               // columns per batch in the y passes of A/C
   int cb;                 // columns per CTA in B
   long long plane;        // n1*n2
+  int accum;              // kernel C adds its result to hpsi instead of storing it (ladd)
 };
 
 __host__ __device__ __forceinline__ int kept_to_idx(int i, int kd, int n, int nk) {

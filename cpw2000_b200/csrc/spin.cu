@@ -144,15 +144,35 @@ __global__ void k_scale_spin_cols(const C2<double>* __restrict__ a, C2<double>* 
   }
 }
 
+// Plane-wave kinetic term hpsi (+)= ekpg psi, one or two components per plane wave
+// (Src/omp/hk_psi_kin_c16.f90).
+__global__ void k_kinetic(int m, int nb, int nspin, const double* __restrict__ ek, const C2<double>* __restrict__ psi,
+                          long long ldpsi, C2<double>* __restrict__ hpsi, long long ldh, int ladd) {
+  const long long rows = (long long)nspin * m, n = rows * nb;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const long long b = t / rows, r = t - b * rows;
+    const double e = ek[r / nspin];
+    const C2<double> x = psi[b * ldpsi + r];
+    C2<double> y = mk<double>(e * x.x, e * x.y);
+    if (ladd) {
+      const C2<double> h0 = hpsi[b * ldh + r];
+      y.x += h0.x;
+      y.y += h0.y;
+    }
+    hpsi[b * ldh + r] = y;
+  }
+}
+
 template <typename T>
 int spin_local(cpw_b200_ctx* c, int nb, const C2<double>* psi, long long ldpsi, C2<double>* hpsi, long long ldh,
-               cudaStream_t st) {
-  const LocalPlan& p = c->plan;
+               cudaStream_t st, bool kinetic = true, int accum = 0) {
+  LocalPlan p = c->plan;
+  p.accum = accum;
   const bool f32 = sizeof(T) == 4;
   const int* ps = (const int*)c->plane_start.p;
   const int* idx2 = (const int*)c->sp_idx2.p;
   const int* pos = (const int*)c->pw_pos.p;
-  const double* ek2 = (const double*)c->sp_ek2.p;
+  const double* ek2 = kinetic ? (const double*)c->sp_ek2.p : nullptr;
   const C2<T>* tw[3];
   for (int a = 0; a < 3; ++a) tw[a] = (const C2<T>*)(f32 ? c->tw32[a].p : c->tw64[a].p);
   const DevBuf* v = f32 ? c->sp_v32 : c->sp_v64;
@@ -262,6 +282,65 @@ int ctx_set_projectors_spin(cpw_b200_ctx* c, int nanl, const double* anlsp, long
                                                  (const double*)dx.p, m2, nanl);
   e = cudaStreamSynchronize(c->stream);
   return e == cudaSuccess ? kOk : cuda_fail(e, "set_projectors_spin");
+}
+
+int ctx_hkpsi_kin_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh,
+                         bool ladd, int nspin, cudaStream_t st) {
+  if (!c->have_basis) return fail(kNotReady, "hk_psi_kin: basis must be set");
+  if (nspin != 1 && nspin != 2) return fail(kBadArg, "hk_psi_kin_c16: nspin should be 1 or 2");
+  if (nb < 0) return fail(kBadArg, "hk_psi_kin: neig < 0");
+  const long long m = c->mtxd;
+  if (nb == 0 || m == 0) return kOk;
+  if (ldpsi < nspin * m || ldh < nspin * m) return fail(kBadArg, "hk_psi_kin: leading dimension smaller than nspin*mtxd");
+  k_kinetic<<<1184, 256, 0, st>>>((int)m, nb, nspin, (const double*)c->ekpg.p, (const C2<double>*)psi, ldpsi,
+                                  (C2<double>*)hpsi, ldh, ladd ? 1 : 0);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? kOk : cuda_fail(e, "hk_psi_kin");
+}
+
+int ctx_hkpsi_loc_general(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh,
+                          bool ladd, int nspin, cudaStream_t st) {
+  if (nspin != 1 && nspin != 2) return fail(kBadArg, "hk_psi_loc_c16: nspin should be 1 or 2");
+  if (!c->have_basis) return fail(kNotReady, "hk_psi_loc: basis must be set");
+  if (nb < 0) return fail(kBadArg, "hk_psi_loc: neig < 0");
+  const long long m = c->mtxd;
+  if (nb == 0 || m == 0) return kOk;
+  if (ldpsi < nspin * m || ldh < nspin * m) return fail(kBadArg, "hk_psi_loc: leading dimension smaller than nspin*mtxd");
+  const C2<double>* x = (const C2<double>*)psi;
+  C2<double>* y = (C2<double>*)hpsi;
+  if (nspin == 2) {
+    if (c->nsp == 0) return fail(kNotReady, "hk_psi_loc: spin potential must be set (cpw_b200_set_potential_spin)");
+    int s;
+    if ((s = c->sp_idx2.ensure((size_t)m * sizeof(int))) || (s = c->sp_ek2.ensure((size_t)2 * m * sizeof(double))))
+      return s;
+    k_double_index<<<592, 256, 0, st>>>((int)m, (const int*)c->pw_idx.p, (const double*)c->ekpg.p,
+                                        (int*)c->sp_idx2.p, (double*)c->sp_ek2.p);
+    return c->precision ? spin_local<float>(c, nb, x, ldpsi, y, ldh, st, false, ladd)
+                        : spin_local<double>(c, nb, x, ldpsi, y, ldh, st, false, ladd);
+  }
+  if (!c->have_pot) return fail(kNotReady, "hk_psi_loc: potential must be set");
+  LocalPlan p = c->plan;
+  p.accum = ladd ? 1 : 0;
+  const bool f32 = c->precision != 0;
+  const size_t per_band = (f32 ? sizeof(C2<float>) : sizeof(C2<double>)) * (size_t)p.nz * (size_t)p.plane;
+  const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nb, c->slab_budget / per_band));
+  if (int s = c->slab.ensure(per_band * (size_t)chunk)) return s;
+  for (int b0 = 0; b0 < nb; b0 += chunk) {
+    const int nbc = std::min(chunk, nb - b0);
+    cudaError_t e;
+    if (f32)
+      e = launch_local<float>(p, nbc, b0, x, ldpsi, y, ldh, (const int*)c->plane_start.p, (const int*)c->pw_idx.p,
+                              (const int*)c->pw_pos.p, nullptr, (const float*)c->v32.p, (const C2<float>*)c->tw32[0].p,
+                              (const C2<float>*)c->tw32[1].p, (const C2<float>*)c->tw32[2].p, (C2<float>*)c->slab.p,
+                              st, nullptr);
+    else
+      e = launch_local<double>(p, nbc, b0, x, ldpsi, y, ldh, (const int*)c->plane_start.p, (const int*)c->pw_idx.p,
+                               (const int*)c->pw_pos.p, nullptr, (const double*)c->v64.p,
+                               (const C2<double>*)c->tw64[0].p, (const C2<double>*)c->tw64[1].p,
+                               (const C2<double>*)c->tw64[2].p, (C2<double>*)c->slab.p, st, nullptr);
+    if (e != cudaSuccess) return cuda_fail(e, "hk_psi_loc local kernels");
+  }
+  return kOk;
 }
 
 int ctx_hkpsi_spin_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh,

@@ -221,6 +221,20 @@ class Context:
         return dict(vscr=vscr[:ident * n2 * n3] if want_vscr else None, vmax=vmax.value, vmin=vmin.value,
                     cmax=cmax.value, kmscr=km)
 
+    def hk_psi_kin(self, psi, hpsi, ladd: bool = False, nspin: int = 1):
+        """hpsi (+)= ekpg psi (Src/omp/hk_psi_kin_c16.f90) on column-major CUDA tensors."""
+        check(self._L.cpw_b200_hk_psi_kin_device(self.handle, int(psi.shape[1]), C.c_void_p(psi.data_ptr()),
+                                                 self._ld(psi), C.c_void_p(hpsi.data_ptr()), self._ld(hpsi),
+                                                 1 if ladd else 0, int(nspin),
+                                                 C.c_void_p(torch_stream_handle(psi.device))))
+
+    def hk_psi_loc(self, psi, hpsi, ladd: bool = False, nspin: int = 1):
+        """hpsi (+)= V_loc psi (Src/omp/hk_psi_loc_c16.f90), nspin 1 or 2 (interleaved spinors)."""
+        check(self._L.cpw_b200_hk_psi_loc_c16_device(self.handle, int(psi.shape[1]), C.c_void_p(psi.data_ptr()),
+                                                     self._ld(psi), C.c_void_p(hpsi.data_ptr()), self._ld(hpsi),
+                                                     1 if ladd else 0, int(nspin),
+                                                     C.c_void_p(torch_stream_handle(psi.device))))
+
     def set_potential_spin(self, vscr_sp, nsp: int):
         """vscr_sp: (mxdscr, nsp) real, columns (1, sigma_z, sigma_x, sigma_y) of the box."""
         v = np.asfortranarray(vscr_sp, dtype=np.float64)

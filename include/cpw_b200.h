@@ -123,6 +123,19 @@ int cpw_b200_pot_local(cpw_b200_ctx* ctx, double* vscr, double* vmax, double* vm
                        const double* phase, const double* conj, int ns, const int* inds, int mxdscr,
                        int mxdgve, int mxdnst, int install);
 
+/* The split operators on device blocks (columns of nspin*mtxd rows, spinor rows
+ * interleaved up, down when nspin = 2), on `stream` (NULL = the context stream);
+ * ladd != 0 adds to hpsi, else hpsi is overwritten:
+ *   cpw_b200_hk_psi_kin_device      replaces Src/omp/hk_psi_kin_c16.f90:22-131
+ *                                   (hpsi (+)= ekpg psi);
+ *   cpw_b200_hk_psi_loc_c16_device  replaces Src/omp/hk_psi_loc_c16.f90:23-362
+ *                                   (local potential alone: the context's vscr when
+ *                                   nspin = 1, its spin potential when nspin = 2). */
+int cpw_b200_hk_psi_kin_device(cpw_b200_ctx* ctx, int neig, const void* psi, long long ldpsi, void* hpsi,
+                               long long ldh, int ladd, int nspin, void* stream);
+int cpw_b200_hk_psi_loc_c16_device(cpw_b200_ctx* ctx, int neig, const void* psi, long long ldpsi, void* hpsi,
+                                   long long ldh, int ladd, int nspin, void* stream);
+
 /* Spinor form on a context (the k-point from cpw_b200_set_kpoint): the nsp
  * potential columns vscr_sp(mxdscr, nsp) (host), the spinor projectors
  * anlsp(ld >= 2*mtxd, nanlsp) and xnlkbsp (host), then hpsi_sp = H psi_sp for

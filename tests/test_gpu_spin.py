@@ -108,3 +108,36 @@ def test_dropin_spin_rejects_bad_nsp(cuda):
                                          iptr(np.ascontiguousarray(d["kmscr"], dtype=np.int32)), iref(3), zptr(anl),
                                          dptr(xnl), iref(xnl.size), iref(m), iref(1), iref(xnl.size), iref(d["ng"]),
                                          iref(vsp.shape[0]), iref(4)))
+
+
+@pytest.mark.parametrize("nspin", [1, 2])
+@pytest.mark.parametrize("ladd", [False, True])
+def test_split_kinetic_and_local_operators(cuda, nspin, ladd):
+    # hk_psi_kin_c16 and hk_psi_loc_c16 on device blocks: T psi and V_loc psi, added or stored
+    import torch
+    nsp = 2 if nspin == 2 else 1
+    d, vsp, anl, xnl = spin_inputs("si2", 2, nsp, seed=11)
+    m, nb = d["mtxd"], 3
+    rows = nspin * m
+    rng = np.random.default_rng(4)
+    psi = rng.standard_normal((rows, nb)) + 1j * rng.standard_normal((rows, nb))
+    h0 = rng.standard_normal((rows, nb)) + 1j * rng.standard_normal((rows, nb))
+    ctx = H.Context(0)
+    ctx.set_kpoint(m, d["isort"], d["kgv"], d["ekpg"], d["kmscr"])
+    ctx.set_potential(d["vscr"])
+    ctx.set_potential_spin(vsp, nsp)
+    x = torch.from_numpy(np.ascontiguousarray(psi.T)).to(cuda).t()
+    base = h0 if ladd else np.zeros_like(h0)
+    ek = np.repeat(np.asarray(d["ekpg"][:m]), nspin)
+    want_kin = base + ek[:, None] * psi
+    none = np.zeros((rows, 0), complex)
+    if nspin == 1:
+        want_loc = base + O.hk_psi_loc(m, nb, psi, d["isort"], d["vscr"], d["kmscr"], d["kgv"])
+    else:
+        want_loc = base + O.hk_psi_spin_c16(m, nb, psi, np.zeros(m), d["isort"], vsp, d["kmscr"], d["kgv"], nsp,
+                                            none, np.zeros(0))
+    for op, want in ((ctx.hk_psi_kin, want_kin), (ctx.hk_psi_loc, want_loc)):
+        y = torch.from_numpy(np.ascontiguousarray(h0.T)).to(cuda).t()
+        op(x, y, ladd=ladd, nspin=nspin)
+        torch.cuda.synchronize()
+        assert relerr(y.cpu().numpy(), want) < TOL64
