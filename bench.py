@@ -166,6 +166,23 @@ def time_to_eigvals(d, local, icmax=300, nocc=128):
     return out
 
 
+def kpoint_eig(local, nk=16, nb=40, workers=16):
+    """Eigensolver over nk k-points of the Si8 cell (Ecut 20 Ha, 40^3, ~4,610 PW, 40 bands):
+    one context after another vs `workers` contexts in flight on host threads
+    (cpw2000_b200.kpoints); the Ritz values of both runs must agree."""
+    from cpw2000_b200 import kpoints
+    w = configs.si8_cubic_kbatch(nk=nk)
+    inputs = [configs.kpoint_inputs(w, k, nbands=nb, with_hamsm=True) for k in range(nk)]
+    kpoints.eigensolve_kpoints(inputs[:2], nb, workers=2, device=local)          # warm-up
+    serial, t1 = kpoints.eigensolve_kpoints(inputs, nb, workers=1, device=local)
+    conc, tn = kpoints.eigensolve_kpoints(inputs, nb, workers=workers, device=local)
+    diff = max(float(np.abs(a["ei"] - b["ei"]).max()) for a, b in zip(serial, conc))
+    return {"workload": f"si8 cubic, Ecut 20 Ha, 40^3 box, {nk} random k-points, {nb} bands, epspsi 1e-5, icmax 60, FP64",
+            "serial_s": t1, "concurrent_s": tn, "workers": workers, "speedup": t1 / tn,
+            "kpoints_per_s": nk / tn, "max_ritz_diff_vs_serial": diff,
+            "converged": int(sum(r["converged"] for r in conc))}
+
+
 def kbatch_throughput(local, steps, warmup, nk=64):
     """Batched H|psi> over the 64 random k-points of the Si8 cubic cell (Ecut 20 Ha, 40^3 box,
     ~4,600 plane waves per k, 40 bands per k): one batched call (autotuned, replayed from a
@@ -509,6 +526,7 @@ def run_ours(args, world, rank, local, dist):
     line["kbatch"] = kbatch_throughput(local, max(3, args.steps // 2), 2)
     if args.eig:
         line["time_to_eigvals"] = time_to_eigvals(d, local)
+        line["kpoint_eig"] = kpoint_eig(local)
     if rank == 0 and world == 1:
         rate, cores = cpu_reference_rate(d, 64, repeats=2)
         line["cpu_baseline"] = {"value": rate, "unit": "bands/s", "cores": cores, "kind": "port",
