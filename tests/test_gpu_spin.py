@@ -141,3 +141,22 @@ def test_split_kinetic_and_local_operators(cuda, nspin, ladd):
         op(x, y, ladd=ladd, nspin=nspin)
         torch.cuda.synchronize()
         assert relerr(y.cpu().numpy(), want) < TOL64
+
+
+@pytest.mark.parametrize("nsp", [2, 4])
+def test_device_spin_box96(cuda, nsp):
+    # the compile-time 96^3 kernels on the component views (nsp 2) and the spinor z stage (nsp 4)
+    import torch
+    d, vsp, anl, xnl = spin_inputs("si64", 0, nsp, nanl=8, seed=20 + nsp)
+    m, nb = d["mtxd"], 3
+    rng = np.random.default_rng(30 + nsp)
+    psi = rng.standard_normal((2 * m, nb)) + 1j * rng.standard_normal((2 * m, nb))
+    ctx = H.Context(0)
+    ctx.set_kpoint(m, d["isort"], d["kgv"], d["ekpg"], d["kmscr"])
+    ctx.set_potential_spin(vsp, nsp)
+    ctx.set_projectors_spin(anl, xnl)
+    x = torch.from_numpy(np.ascontiguousarray(psi.T)).to(cuda).t()
+    y = torch.zeros((nb, 2 * m), dtype=torch.complex128, device=cuda).t()
+    ctx.hk_psi_spin(x, y)
+    torch.cuda.synchronize()
+    assert relerr(y.cpu().numpy(), oracle(d, psi, nb, vsp, nsp, anl, xnl)) < TOL64
