@@ -680,8 +680,23 @@ int tc_nl_apply_ops(TcScratch& t, int m, int na, long long nkb1, long long nkb2,
 
   // GEMM 1: (2 nanl) x nb, K = 2 mtxd, split over K so that the work items fill the SMs about once
   const int mt1 = (2 * na + tc::BM - 1) / tc::BM, nt1 = (nb + tc::BN - 1) / tc::BN;
-  // splits: 0 = about one work item per SM, > 0 that many, -d a d-th of the default
-  int nsplit = std::max(1, (int)std::min<long long>(nkb1, nsm / (mt1 * nt1)));
+  // splits: 0 = the split with the fewest waves per unit of K (ceil(tiles s / nsm) / s, a
+  // smaller s unless a larger one is 3% better: Si64 8 tiles -> 18 splits, one wave; Si216
+  // 56 tiles -> 21 splits, 8 waves at 99% of the SMs instead of 2 splits on 112 of 148),
+  // > 0 that many, -d a d-th of the default
+  int nsplit = 1;
+  {
+    const long long tiles = (long long)mt1 * nt1;
+    const long long smax = std::max(1LL, std::min<long long>(nkb1, 16LL * nsm / tiles + 1));
+    double best = 1e300;
+    for (long long sp = 1; sp <= smax; ++sp) {
+      const double cost = (double)((tiles * sp + nsm - 1) / nsm) / (double)sp;
+      if (cost < best * 0.97) {
+        best = cost;
+        nsplit = (int)sp;
+      }
+    }
+  }
   if (splits < 0) nsplit = std::max(1, nsplit / -splits);
   if (splits > 0) nsplit = (int)std::min<long long>(nkb1, splits);
   if (const int ks = env_int("CPW_B200_TC_SPLITS", 0)) nsplit = (int)std::max(1LL, std::min<long long>(nkb1, ks));
