@@ -88,6 +88,7 @@ int d2h_cols(double* dst, long long ldd, const void* src, long long lds, long lo
 struct DropinPipe {
   int m = 0, nb = 0, chunk = 0, nchunk = 0;
   long long ldh = 0;
+  std::vector<int> start;     // band boundaries of the chunks (nchunk + 1)
 };
 
 int dropin_stage_in(cpw_b200_ctx* c, int m, int nb, const double* psi, long long ldh_host, DropinPipe* pp) {
@@ -100,6 +101,18 @@ int dropin_stage_in(cpw_b200_ctx* c, int m, int nb, const double* psi, long long
   p.ldh = ldh_host;
   p.chunk = std::max(kMinChunk, (nb + kChunks - 1) / kChunks);
   p.nchunk = (nb + p.chunk - 1) / p.chunk;
+  // the first chunk's copy-in and the last chunk's copy-out are the transfers no compute hides:
+  // with 3 or more chunks those two are half the size of the others (CPW_B200_DROPIN_EVEN=1:
+  // equal chunks)
+  p.start.assign(1, 0);
+  const char* even = getenv("CPW_B200_DROPIN_EVEN");
+  if (p.nchunk >= 3 && !(even && atoi(even))) {
+    const double unit = (double)nb / (p.nchunk - 1);
+    for (int k = 1; k < p.nchunk; ++k) p.start.push_back((int)lround(unit * (k - 0.5)));
+  } else {
+    for (int k = 1; k < p.nchunk; ++k) p.start.push_back(k * p.chunk);
+  }
+  p.start.push_back(nb);
   cudaError_t e;
   if (!c->s_in && (e = cudaStreamCreateWithFlags(&c->s_in, cudaStreamNonBlocking)) != cudaSuccess)
     return cuda_fail(e, "hk_psi_c16 stream");
@@ -116,7 +129,7 @@ int dropin_stage_in(cpw_b200_ctx* c, int m, int nb, const double* psi, long long
     return cuda_fail(e, "hk_psi_c16 pipeline");
   C2d* din = (C2d*)c->h_in.p;
   for (int k = 0; k < p.nchunk; ++k) {
-    const int b0 = k * p.chunk, nbc = std::min(p.chunk, nb - b0);
+    const int b0 = p.start[k], nbc = p.start[k + 1] - b0;
     if (int s = h2d_cols(din + (size_t)b0 * m, m, psi + 2 * (size_t)b0 * ldh_host, ldh_host, m, nbc, c->s_in)) return s;
     if ((e = cudaEventRecord(c->ev_pipe[2 * k], c->s_in)) != cudaSuccess) return cuda_fail(e, "hk_psi_c16 pipeline");
   }
@@ -168,7 +181,7 @@ int dropin_compute_out(cpw_b200_ctx* c, const DropinPipe& p, double* hpsi, bool 
   }
   const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
   for (int k = 0; k < p.nchunk; ++k) {
-    const int b0 = k * p.chunk, nbc = std::min(p.chunk, p.nb - b0);
+    const int b0 = p.start[k], nbc = p.start[k + 1] - b0;
     cudaEvent_t in_done = c->ev_pipe[2 * k], out_ready = c->ev_pipe[2 * k + 1];
     if ((e = cudaStreamWaitEvent(c->stream, in_done, 0)) != cudaSuccess) return cuda_fail(e, "hk_psi_c16 pipeline");
     if (split_nl) {
