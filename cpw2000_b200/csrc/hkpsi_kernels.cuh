@@ -24,6 +24,11 @@ constexpr int pass_threads(int lines_a, int lines_b) {
 }
 // CTAs per SM asked of the register allocator: two CTAs of 384 threads fit in 80 registers.
 constexpr int pass_min_blocks(int nt) { return nt == 384 ? 2 : 1; }
+// Kernels A and C: FP64 planes of 128 points or more take over 200 KB of shared memory (one CTA
+// per SM whatever the registers), so they get no register cap.
+template <typename T> constexpr int plane_min_blocks(int nt, int n1) {
+  return sizeof(T) == 8 && n1 >= 128 ? 1 : pass_min_blocks(nt);
+}
 
 template <typename T> __device__ __forceinline__ C2<T> czero() { return mk<T>(T(0), T(0)); }
 
@@ -31,7 +36,7 @@ template <typename T> __device__ __forceinline__ C2<T> czero() { return mk<T>(T(
 // A: scatter + inverse x + inverse y, one CTA per (band, kept z-plane)
 // ---------------------------------------------------------------------------
 template <typename T, int RX1, int RX2, int RY1, int RY2, int TC, int NT = kThreadsPlanes>
-__global__ void __launch_bounds__(NT, pass_min_blocks(NT))
+__global__ void __launch_bounds__(NT, plane_min_blocks<T>(NT, RX1 * RX2))
 k_inv_xy(LocalPlan p, int band0, const C2<double>* __restrict__ psi, long long ldpsi,
          const int* __restrict__ plane_start, const int* __restrict__ pw_idx,
          const int* __restrict__ pw_pos, const C2<T>* __restrict__ twx,
@@ -388,7 +393,7 @@ k_z_vloc_pipe(LocalPlan p, int nbc, int bands_per_group, const T* __restrict__ v
 // C: forward y + forward x + gather + kinetic, one CTA per (band, kept z-plane)
 // ---------------------------------------------------------------------------
 template <typename T, int RX1, int RX2, int RY1, int RY2, int TC, int NT = kThreadsPlanes>
-__global__ void __launch_bounds__(NT, pass_min_blocks(NT))
+__global__ void __launch_bounds__(NT, plane_min_blocks<T>(NT, RX1 * RX2))
 k_fwd_xy(LocalPlan p, int band0, const C2<double>* __restrict__ psi, long long ldpsi,
          C2<double>* __restrict__ hpsi, long long ldh, const int* __restrict__ plane_start,
          const int* __restrict__ pw_idx, const int* __restrict__ pw_pos,
@@ -541,9 +546,8 @@ cudaError_t launch_impl(const LocalPlan& p, int nbc, int band0, const C2<double>
                         const C2<T>* twz, C2<T>* W, cudaStream_t st, cudaEvent_t* ev) {
   constexpr int NTP = TC && RY1 ? pass_threads(TC * RY2, TC * RY1) : kThreadsPlanes;
   constexpr int NTZ = CB && RZ1 ? pass_threads(CB * RZ2, CB * RZ1) : kThreadsCols;
-  // C keeps 256 threads where 384 measured slower: FP64 on 144-point lines (the 80-register
-  // cap spills) and FP32 on 96-point lines.
-  constexpr bool c_wide = sizeof(T) == 8 ? RY1 * RY2 < 128 : RY1 * RY2 >= 128;
+  // C keeps 256 threads where 384 measured slower: FP32 on 96-point lines.
+  constexpr bool c_wide = sizeof(T) == 8 || RY1 * RY2 >= 128;
   constexpr int NTC = NTP == 384 && c_wide ? 384 : kThreadsPlanes;
   const size_t sm_pl = smem_planes<T>(p);
   auto* ka = k_inv_xy<T, RX1, RX2, RY1, RY2, TC, NTP>;
