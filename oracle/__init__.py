@@ -20,8 +20,8 @@ fft      -- Src/fft/_cfft/cfft_wf_c16.f pruned 3D FFT (conventions and pruning)
 hk_psi   -- Src/hk_psi/reference/hk_psi_c16.f90, hk_psi_spin_c16.f90 (spinors),
             Src/cpw_lib/hk_psi_nl_c16.f90
 ditsp    -- Src/ditsp/*.f90, Src/omp/diag_rq_jac_c16.f90, Src/numeric/ran2.f90
-density  -- Src/omp/charge_by_fft.f90
-forces   -- Src/ALFA/for_str_nl_kb.f90, Src/ALFA/for_str_local_force.f90
+forces   -- Src/ALFA/for_str_nl_kb.f90, Src/ALFA/for_str_local_force.f90, and the density
+            Src/omp/charge_by_fft.f90
 stress   -- Src/ALFA/for_str_kinetic_stress.f90, for_str_local_stress.f90, for_str_nl_kb.f90 (stress)
 c/       -- C + OpenMP restatement of hk_psi_c16 (CPU baseline timing)
 """
