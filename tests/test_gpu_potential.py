@@ -98,3 +98,11 @@ def test_installed_potential_drives_hpsi(cuda, prec):
     ctx.hk_psi(x, y)
     torch.cuda.synchronize()
     assert relerr(y.cpu().numpy(), y_ref.cpu().numpy()) < (1e-12 if prec == H.FP64 else 1e-6)
+
+
+def test_empty_star_list_gives_zero_potential(cuda):
+    w = workload("si2")
+    km = [(n - 1) // 2 for n in w.box]
+    r = H.Context(0).pot_local(np.zeros(1, complex), np.zeros((3, 0), np.int32), np.zeros(0, np.int32), kmscr=km,
+                               install=False)
+    assert np.all(r["vscr"] == 0.0) and r["cmax"] == 0.0 and r["vmax"] == 0.0 and r["vmin"] == 0.0

@@ -118,3 +118,25 @@ def _call_with_nanl(ctx, d, w, nkb, nanl):
                                             iptr(np.full(ntype, nq, dtype=np.int32)),
                                             dptr(np.full(ntype, 0.01)), dptr(vref), nq, iptr(nref), int(nanl), None,
                                             None, 0))
+
+
+def test_no_projectors(cuda):
+    # species without KB channels: nanl = 0, H|psi> then has no non-local term
+    import torch
+    w = configs.WORKLOADS["si2"]()
+    d = configs.kpoint_inputs(w, 0)
+    nkb = np.zeros_like(np.asarray(d["nkb"]))
+    ctx = H.Context(0)
+    ctx.set_kpoint(d["mtxd"], d["isort"], d["kgv"], d["ekpg"], d["kmscr"])
+    ctx.set_potential(d["vscr"])
+    xnl = ctx.proj_nl_kb(d["rkpt"], w.species, d["vkb"], nkb, w.adot)
+    assert xnl.size == 0 and ctx.nanl == 0
+    psi = configs.random_psi(d["mtxd"], 3, 1)
+    x = torch.from_numpy(np.ascontiguousarray(psi.T)).to(cuda).t()
+    y = torch.zeros((3, d["mtxd"]), dtype=torch.complex128, device=cuda).t()
+    ctx.hk_psi(x, y)
+    torch.cuda.synchronize()
+    from oracle import hk_psi as O
+    want = O.hk_psi_c16(d["mtxd"], 3, psi, d["ekpg"], d["isort"], d["vscr"], d["kmscr"], d["kgv"],
+                        np.zeros((d["mtxd"], 0), complex), np.zeros(0))
+    assert relerr(y.cpu().numpy(), want) < TOL
