@@ -309,6 +309,8 @@ int cpw_b200_destroy(cpw_b200_ctx* c) {
   if (c->s_nl) cudaStreamSynchronize(c->s_nl);
   for (cudaEvent_t e : c->ev_pipe) cudaEventDestroy(e);
   for (cudaEvent_t e : c->ev_nl) cudaEventDestroy(e);
+  for (cudaEvent_t e : c->ov_ev)
+    if (e) cudaEventDestroy(e);
   if (c->s_in) cudaStreamDestroy(c->s_in);
   if (c->s_out) cudaStreamDestroy(c->s_out);
   if (c->blas_nl) cublasDestroy(c->blas_nl);

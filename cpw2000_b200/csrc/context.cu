@@ -305,6 +305,44 @@ int ctx_hkpsi_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, 
   const C2<double>* ps = (const C2<double>*)psi;
   C2<double>* hp = (C2<double>*)hpsi;
   const double* ek = with_kinetic ? (const double*)c->ekpg.p : nullptr;
+  // FP64 projector products: the projection P = X^H psi needs psi only, so it runs on the
+  // projection stream beside the local kernels (filling the SMs their tails leave idle); the
+  // expansion follows the local kernels on st. CPW_B200_NL_OVERLAP=0 keeps both on st.
+  const bool cublas_nl = with_nl && c->nanl > 0 && !(c->precision == 2 && c->tc_ready);
+  bool overlap = false;
+  cudaEvent_t ov_t0 = nullptr, ov_t1 = nullptr;
+  if (cublas_nl) {
+    const char* v = getenv("CPW_B200_NL_OVERLAP");
+    overlap = !(v && atoi(v) == 0);
+  }
+  if (overlap) {
+    cudaError_t e;
+    if (!c->s_nl && (e = cudaStreamCreateWithFlags(&c->s_nl, cudaStreamNonBlocking)) != cudaSuccess)
+      return cuda_fail(e, "hk_psi stream");
+    if (!c->blas_nl) {
+      if (cublasCreate(&c->blas_nl) != CUBLAS_STATUS_SUCCESS) {
+        c->blas_nl = nullptr;
+        return fail(kCublas, "cublasCreate failed");
+      }
+    }
+    for (auto& ev : c->ov_ev)
+      if (!ev && (e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return cuda_fail(e, "event");
+    if ((s = c->proj.ensure((size_t)c->nanl * nb * sizeof(C2<double>)))) return s;
+    if ((e = cudaEventRecord(c->ov_ev[0], st)) != cudaSuccess || (e = cudaStreamWaitEvent(c->s_nl, c->ov_ev[0], 0)) != cudaSuccess)
+      return cuda_fail(e, "hk_psi overlap");
+    ov_t0 = c->timer.on ? c->timer.take() : nullptr;
+    ov_t1 = c->timer.on ? c->timer.take() : nullptr;
+    if (ov_t0) cudaEventRecord(ov_t0, c->s_nl);
+    cublasSetStream(c->blas_nl, c->s_nl);
+    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+    // P = X^H psi (hk_psi_nl_c16.f90:82)
+    if (cublasZgemm(c->blas_nl, CUBLAS_OP_C, CUBLAS_OP_N, c->nanl, nb, c->mtxd, &one, (const cuDoubleComplex*)c->anl.p,
+                    c->mtxd, (const cuDoubleComplex*)psi, (int)ldpsi, &zero, (cuDoubleComplex*)c->proj.p,
+                    c->nanl) != CUBLAS_STATUS_SUCCESS)
+      return fail(kCublas, "zgemm X^H psi");
+    if (ov_t1) cudaEventRecord(ov_t1, c->s_nl);
+    if ((e = cudaEventRecord(c->ov_ev[1], c->s_nl)) != cudaSuccess) return cuda_fail(e, "hk_psi overlap");
+  }
   for (int b0 = 0; b0 < nb; b0 += chunk) {
     const int nbc = std::min(chunk, nb - b0);
     cudaError_t e;
@@ -331,6 +369,23 @@ int ctx_hkpsi_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, 
       c->timer.mark(kStZVloc, ev[1], ev[2]);
       c->timer.mark(kStFwdXY, ev[2], ev[3]);
     }
+  }
+  if (overlap) {
+    cudaError_t e;
+    if ((e = cudaStreamWaitEvent(st, c->ov_ev[1], 0)) != cudaSuccess) return cuda_fail(e, "hk_psi overlap");
+    cudaEvent_t t1 = c->timer.on ? c->timer.take() : nullptr, t2 = c->timer.on ? c->timer.take() : nullptr;
+    if (t1) cudaEventRecord(t1, st);
+    cublasSetStream(c->blas, st);
+    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
+    // hpsi += (X D) P (hk_psi_nl_c16.f90:87-96)
+    if (cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, c->mtxd, nb, c->nanl, &one, (const cuDoubleComplex*)c->anld.p,
+                    c->mtxd, (const cuDoubleComplex*)c->proj.p, c->nanl, &one, (cuDoubleComplex*)hpsi,
+                    (int)ldh) != CUBLAS_STATUS_SUCCESS)
+      return fail(kCublas, "zgemm X D P");
+    if (t2) cudaEventRecord(t2, st);
+    c->timer.mark(kStNlProj, ov_t0, ov_t1);
+    c->timer.mark(kStNlExpand, t1, t2);
+    return kOk;
   }
   if (with_nl && c->nanl > 0) {
     if ((s = c->proj.ensure((size_t)c->nanl * nb * sizeof(C2<double>)))) return s;

@@ -106,6 +106,7 @@ struct cpw_b200_ctx {
   cudaStream_t s_nl = nullptr;
   cublasHandle_t blas_nl = nullptr;
   std::vector<cudaEvent_t> ev_nl;
+  cudaEvent_t ov_ev[2] = {nullptr, nullptr};   // device H|psi>: projection on s_nl beside the local kernels
   cublasHandle_t blas = nullptr;
   int precision = 0;            // 0: FP64; 1: FP32 local + FP64 projector GEMMs; 2: 1 with split-TF32 tensor-core projectors
   size_t slab_budget = 512ull << 20;
