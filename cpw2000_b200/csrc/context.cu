@@ -305,15 +305,17 @@ int ctx_hkpsi_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, 
   const C2<double>* ps = (const C2<double>*)psi;
   C2<double>* hp = (C2<double>*)hpsi;
   const double* ek = with_kinetic ? (const double*)c->ekpg.p : nullptr;
-  // FP64 projector products: the projection P = X^H psi needs psi only, so it runs on the
-  // projection stream beside the local kernels (filling the SMs their tails leave idle); the
-  // expansion follows the local kernels on st. CPW_B200_NL_OVERLAP=0 keeps both on st.
+  // FP64 projector products of the MIXED form: the projection P = X^H psi needs psi only, so it
+  // runs on the projection stream beside the FP32 local kernels (filling the SMs their tails leave
+  // idle; Si216 28.5 -> 27.7 ms); the expansion follows the local kernels on st. The FP64 form
+  // gains 0.5-1% this way and keeps both on st, so that its stage timers time each kernel alone.
+  // CPW_B200_NL_OVERLAP=1 / 0 forces either way.
   const bool cublas_nl = with_nl && c->nanl > 0 && !(c->precision == 2 && c->tc_ready);
   bool overlap = false;
   cudaEvent_t ov_t0 = nullptr, ov_t1 = nullptr;
   if (cublas_nl) {
     const char* v = getenv("CPW_B200_NL_OVERLAP");
-    overlap = !(v && atoi(v) == 0);
+    overlap = v ? atoi(v) != 0 : c->precision == 1;
   }
   if (overlap) {
     cudaError_t e;
