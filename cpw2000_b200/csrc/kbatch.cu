@@ -7,8 +7,9 @@
 // lists and kinetic diagonal relative to it, and the local kernels A and C read a
 // per-band table (k-point, band) and a per-k descriptor, so one launch per stage
 // covers all k-points and uneven plane-wave counts and band counts (kernel B only
-// sees slabs). The projector products follow per k-point (each k has its own X):
-// cuBLAS ZGEMMs in FP64 / MIXED, the split-TF32 tensor-core kernels in MIXED_TC.
+// sees slabs). The projector products (each k has its own X) run for all k-points in three
+// launches when the blocks are small (FP64 / MIXED, below), else per k-point: cuBLAS ZGEMMs in
+// FP64 / MIXED, the split-TF32 tensor-core kernels in MIXED_TC.
 //
 // The first call for a given set of arrays and band counts autotunes the launch
 // shape (slab chunk size, kernel B band grouping, split count of the tensor-core
@@ -42,6 +43,11 @@ struct cpw_b200_kbatch {
   std::vector<long long> nkb1, nkb2;
   std::vector<char> tc_ready;
   DevBuf kdesc_d, bref_d, proj, blas_ws, slab;
+  // projector products of all k-points in three launches (FP64 / MIXED, small blocks)
+  DevBuf nl_d, nl_part;
+  bool nl_batched = false;
+  long long nl_ptot = 0;
+  int nl_mmax = 0;
   cpwb::TcScratch tcs;    // own scratch: a captured call keeps these pointers
   cudaStream_t st = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr, t0 = nullptr, t1 = nullptr;
@@ -79,6 +85,121 @@ struct Call {
   int total = 0;
 };
 
+// Projector products of every k-point of the batch at once (FP64 / MIXED), for blocks of at
+// most kNlMax projectors and kNlMax bands per k-point. Per k-point ZGEMMs of a few dozen
+// projectors and bands are latency-bound launches (two per k-point, one after the other); here
+//   k_batch_proj:   partial P_k = X_k^H psi_k over a slice of plane waves, per (k, slice)
+//   k_batch_reduce: P_k = sum of the slices, times nothing (xnlkb sits in X D)
+//   k_batch_expand: hpsi_k += (X D)_k P_k, one thread per plane wave of each k
+// (hk_psi_nl_c16.f90:82-96), in a fixed order: the result does not depend on timing.
+struct NlDesc {
+  const C2<double>* x;
+  const C2<double>* xd;
+  int m, na, nb;
+  long long poff;      // offset of P_k (na x nb) in the concatenated P
+};
+constexpr int kNlMax = 64, kNlSlices = 8, kNlRows = 16, kNlThreads = 256;
+constexpr int kNlPer = kNlMax * kNlMax / kNlThreads;   // outputs per thread
+constexpr int kNlSmem = kNlMax * kNlMax * (int)sizeof(C2<double>);
+
+__global__ void __launch_bounds__(kNlThreads)
+k_batch_proj(const NlDesc* __restrict__ nd, const KDesc* __restrict__ kd, C2<double>* __restrict__ part,
+             long long ptot) {
+  __shared__ C2<double> xs[kNlRows][kNlMax], ps[kNlRows][kNlMax];
+  const NlDesc D = nd[blockIdx.x];
+  if (D.na == 0 || D.nb == 0 || D.m == 0) return;
+  const C2<double>* psi = kd[blockIdx.x].psi;
+  const long long ldpsi = kd[blockIdx.x].ldpsi;
+  const int per = (D.m + kNlSlices - 1) / kNlSlices;
+  const int r0 = blockIdx.y * per, r1 = min(D.m, r0 + per);
+  const int nout = D.na * D.nb, tid = threadIdx.x;
+  C2<double> acc[kNlPer];
+#pragma unroll
+  for (int t = 0; t < kNlPer; ++t) acc[t] = cpwb::mk<double>(0.0, 0.0);
+  for (int i0 = r0; i0 < r1; i0 += kNlRows) {
+    const int nr = min(kNlRows, r1 - i0);
+    __syncthreads();
+    for (int it = tid; it < kNlRows * kNlMax; it += kNlThreads) {
+      const int r = it % kNlRows, c = it / kNlRows;
+      const bool in = r < nr;
+      xs[r][c] = in && c < D.na ? D.x[(size_t)c * D.m + i0 + r] : cpwb::mk<double>(0.0, 0.0);
+      ps[r][c] = in && c < D.nb ? psi[(size_t)c * ldpsi + i0 + r] : cpwb::mk<double>(0.0, 0.0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < kNlPer; ++t) {
+      const int o = tid + t * kNlThreads;
+      if (o < nout) {
+        const int j = o % D.na, n = o / D.na;
+        C2<double> a = acc[t];
+#pragma unroll 4
+        for (int r = 0; r < kNlRows; ++r) {
+          const C2<double> xv = xs[r][j], pv = ps[r][n];
+          // conj(x) * psi
+          a.x = fma(xv.x, pv.x, fma(xv.y, pv.y, a.x));
+          a.y = fma(xv.x, pv.y, fma(-xv.y, pv.x, a.y));
+        }
+        acc[t] = a;
+      }
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < kNlPer; ++t) {
+    const int o = tid + t * kNlThreads;
+    if (o < nout) part[(size_t)blockIdx.y * ptot + D.poff + o] = acc[t];
+  }
+}
+
+__global__ void k_batch_reduce(const C2<double>* __restrict__ part, C2<double>* __restrict__ P, long long ptot) {
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < ptot; o += (long long)gridDim.x * blockDim.x) {
+    C2<double> a = part[o];
+    for (int sl = 1; sl < kNlSlices; ++sl) {
+      const C2<double> b = part[(size_t)sl * ptot + o];
+      a.x += b.x;
+      a.y += b.y;
+    }
+    P[o] = a;
+  }
+}
+
+__global__ void __launch_bounds__(128)
+k_batch_expand(const NlDesc* __restrict__ nd, const KDesc* __restrict__ kd, const C2<double>* __restrict__ P) {
+  extern __shared__ __align__(16) unsigned char nl_smem[];
+  C2<double>* pk = reinterpret_cast<C2<double>*>(nl_smem);   // P_k, na x nb
+  const NlDesc D = nd[blockIdx.y];
+  if (D.na == 0 || D.nb == 0 || D.m == 0) return;
+  for (int o = threadIdx.x; o < D.na * D.nb; o += blockDim.x) pk[o] = P[D.poff + o];
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= D.m) return;
+  C2<double>* hp = kd[blockIdx.y].hpsi;
+  const long long ldh = kd[blockIdx.y].ldh;
+  constexpr int kB = 8;
+  for (int n0 = 0; n0 < D.nb; n0 += kB) {
+    C2<double> acc[kB];
+#pragma unroll
+    for (int t = 0; t < kB; ++t) acc[t] = cpwb::mk<double>(0.0, 0.0);
+    for (int j = 0; j < D.na; ++j) {
+      const C2<double> x = D.xd[(size_t)j * D.m + i];
+#pragma unroll
+      for (int t = 0; t < kB; ++t) {
+        if (n0 + t < D.nb) {
+          const C2<double> p = pk[j + (n0 + t) * D.na];
+          acc[t].x = fma(x.x, p.x, fma(-x.y, p.y, acc[t].x));
+          acc[t].y = fma(x.x, p.y, fma(x.y, p.x, acc[t].y));
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < kB; ++t)
+      if (n0 + t < D.nb) {
+        C2<double>& h = hp[(size_t)(n0 + t) * ldh + i];
+        h.x += acc[t].x;
+        h.y += acc[t].y;
+      }
+  }
+}
+
 // one pass of the batched H|psi> with a given launch shape, on b->st (capturable: no
 // allocation or host synchronisation once the buffers exist)
 int run_once(cpw_b200_kbatch* b, const Call& call, int chunk, int bgroups, int splits) {
@@ -107,6 +228,17 @@ int run_once(cpw_b200_kbatch* b, const Call& call, int chunk, int bgroups, int s
                                      (const C2<double>*)c->tw64[1].p, (const C2<double>*)c->tw64[2].p,
                                      (C2<double>*)b->slab.p, b->st, nullptr);
     if (e != cudaSuccess) return cuda_fail(e, "kbatch local kernels");
+  }
+  if (b->nl_batched) {
+    const NlDesc* nd = (const NlDesc*)b->nl_d.p;
+    const KDesc* kd = (const KDesc*)b->kdesc_d.p;
+    C2<double>* part = (C2<double>*)b->nl_part.p;
+    C2<double>* P = (C2<double>*)b->proj.p;
+    k_batch_proj<<<dim3(b->nk, kNlSlices), kNlThreads, 0, b->st>>>(nd, kd, part, b->nl_ptot);
+    k_batch_reduce<<<296, 256, 0, b->st>>>(part, P, b->nl_ptot);
+    k_batch_expand<<<dim3((b->nl_mmax + 127) / 128, b->nk), 128, kNlSmem, b->st>>>(nd, kd, P);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? cpwb::kOk : cuda_fail(e, "kbatch projector kernels");
   }
   const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
   for (int k = 0; k < b->nk; ++k) {
@@ -305,6 +437,38 @@ int cpw_b200_kbatch_hk_psi_device(cpw_b200_kbatch* b, const int* nb, void* const
         (s = b->proj.ensure(std::max<size_t>(maxproj, 1) * sizeof(C2<double>))) ||
         (s = b->blas_ws.ensure(kBlasWorkspace)))
       return s;
+    // all projector products in three launches when every block is small (FP64 / MIXED);
+    // CPW_B200_KBATCH_NL=0 keeps one ZGEMM pair per k-point
+    {
+      const char* v = getenv("CPW_B200_KBATCH_NL");
+      bool small = b->precision != 2 && !(v && atoi(v) == 0);
+      std::vector<NlDesc> nd(b->nk);
+      long long poff = 0;
+      int mmax = 0;
+      for (int k = 0; k < b->nk && small; ++k) {
+        const int na = b->nanl[k], nbk = std::max(nb[k], 0), m = b->mtxd[k];
+        if (na > kNlMax || nbk > kNlMax) small = false;
+        nd[k].x = (const C2<double>*)b->anl[k].p;
+        nd[k].xd = (const C2<double>*)b->anld[k].p;
+        nd[k].m = (na > 0 && nbk > 0) ? m : 0;
+        nd[k].na = na;
+        nd[k].nb = nbk;
+        nd[k].poff = poff;
+        poff += (long long)na * nbk;
+        mmax = std::max(mmax, m);
+      }
+      b->nl_batched = small && poff > 0;
+      if (b->nl_batched) {
+        b->nl_ptot = poff;
+        b->nl_mmax = mmax;
+        cudaError_t ea = cudaFuncSetAttribute(k_batch_expand, cudaFuncAttributeMaxDynamicSharedMemorySize, kNlSmem);
+        if (ea != cudaSuccess) return cuda_fail(ea, "kbatch attribute");
+        if ((s = cpwb::upload(b->nl_d, nd.data(), nd.size() * sizeof(NlDesc))) ||
+            (s = b->nl_part.ensure((size_t)kNlSlices * poff * sizeof(C2<double>))) ||
+            (s = b->proj.ensure((size_t)poff * sizeof(C2<double>))))
+          return s;
+      }
+    }
     cublasSetStream(c->blas, b->st);
     cublasSetWorkspace(c->blas, b->blas_ws.p, kBlasWorkspace);
     // slab memory for all bands at once, within the context's slab budget
