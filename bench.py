@@ -166,7 +166,7 @@ def time_to_eigvals(d, local, icmax=300, nocc=128):
     return out
 
 
-def kpoint_eig(local, nk=16, nb=40, workers=16):
+def kpoint_eig(local, nk=16, nb=40, workers=8):
     """Eigensolver over nk k-points of the Si8 cell (Ecut 20 Ha, 40^3, ~4,610 PW, 40 bands):
     one context after another vs `workers` contexts in flight on host threads
     (cpw2000_b200.kpoints); the Ritz values of both runs must agree."""

@@ -315,6 +315,7 @@ int cpw_b200_destroy(cpw_b200_ctx* c) {
   if (c->s_out) cudaStreamDestroy(c->s_out);
   if (c->blas_nl) cublasDestroy(c->blas_nl);
   if (c->s_nl) cudaStreamDestroy(c->s_nl);
+  ditsp_release(c);
   if (c->blas) cublasDestroy(c->blas);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;

@@ -142,6 +142,10 @@ struct cpw_b200_ctx {
   int nanl_sp = 0;
   cpwb::DevBuf anl_sp, anld_sp, sp_idx2, sp_ek2;
 
+  // eigensolver device buffers and cuSOLVER handle, kept between calls (ditsp.cu)
+  cpwb::DevBuf ditsp_pool[20];
+  void* ditsp_sol = nullptr;
+
   cpwb::StageTimer timer;
 
   // slab for the band chunk and staging for host-array entry points
@@ -158,6 +162,7 @@ int ctx_set_basis(cpw_b200_ctx* c, int mtxd, const int* isort, const int* kgv, i
                   const int* kmscr);
 int ctx_set_potential(cpw_b200_ctx* c, const double* vscr, long long nscr);
 int ctx_set_projectors(cpw_b200_ctx* c, int nanl, const double* anlga, int ld, const double* xnlkb, bool on_device);
+void ditsp_release(cpw_b200_ctx* c);
 int ctx_set_potential_spin(cpw_b200_ctx* c, const double* vscr_sp, long long mxdscr, int nsp);
 int ctx_set_projectors_spin(cpw_b200_ctx* c, int nanl, const double* anlsp, long long ld, const double* xnlkb);
 int ctx_hkpsi_kin_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh,

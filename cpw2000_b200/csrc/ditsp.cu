@@ -733,6 +733,34 @@ struct Solver {
   }
 };
 
+// The solver's device buffers and cuSOLVER handle live in the context between calls: allocating
+// and freeing them per call costs milliseconds and cudaFree synchronises the whole device, which
+// would serialise contexts that solve different k-points at the same time.
+struct SolverPool {
+  Solver& S;
+  DevBuf* m[20];
+  explicit SolverPool(Solver& s) : S(s) {
+    DevBuf* l[20] = {&S.bas,  &S.hbas,      &S.smallA,    &S.smallV,   &S.dvec,     &S.dvec2,    &S.dz,
+                     &S.work, &S.info,      &S.eg_d,      &S.hdiag_d,  &S.ham_prev, &S.chol_g,   &S.chol_work,
+                     &S.chol_info, &S.chol_idx, &S.mgs_part, &S.mgs_bar, &S.mgs_irow, &S.mgs_xscl};
+    for (int i = 0; i < 20; ++i) {
+      m[i] = l[i];
+      swap(*m[i], S.c->ditsp_pool[i]);
+    }
+    S.sol = (cusolverDnHandle_t)S.c->ditsp_sol;
+    if (S.sol) cusolverDnSetStream(S.sol, S.st);
+  }
+  ~SolverPool() {
+    for (int i = 0; i < 20; ++i) swap(*m[i], S.c->ditsp_pool[i]);
+    S.c->ditsp_sol = (void*)S.sol;
+    S.sol = nullptr;
+  }
+  static void swap(DevBuf& a, DevBuf& b) {
+    std::swap(a.p, b.p);
+    std::swap(a.bytes, b.bytes);
+  }
+};
+
 struct Trim {
   std::vector<double>* eg;
   int nconv, niter;
@@ -787,6 +815,7 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
   S.P = (Z*)psi;
   S.HP = (Z*)hpsi;
   S.timing = ipr > 1;
+  SolverPool pool(S);
   // in-block orthonormalisation: the reference's recursive Gram-Schmidt for the FP64 drop-in,
   // Cholesky QR twice for the mixed form; CPW_B200_ORTHO=mgs|cholqr overrides
   S.chol = c->precision != 0;
@@ -1315,10 +1344,13 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
            S.tphase[5], S.tphase[6], S.tphase[7], S.tphase[8], S.ham_reused, S.ham_full, S.tphase[9]);
     fflush(stdout);
   }
-  if (S.sol) cusolverDnDestroy(S.sol);
-  S.sol = nullptr;
   if ((s = S.ck(cudaStreamSynchronize(st), "ditsp"))) return s;
   return lconv ? kOk : kNotConverged;
+}
+
+void ditsp_release(cpw_b200_ctx* c) {
+  if (c->ditsp_sol) cusolverDnDestroy((cusolverDnHandle_t)c->ditsp_sol);
+  c->ditsp_sol = nullptr;
 }
 
 }  // namespace cpwb
