@@ -8,8 +8,9 @@
 // per-band table (k-point, band) and a per-k descriptor, so one launch per stage
 // covers all k-points and uneven plane-wave counts and band counts (kernel B only
 // sees slabs). The projector products (each k has its own X) run for all k-points in three
-// launches when the blocks are small (FP64 / MIXED, below), else per k-point: cuBLAS ZGEMMs in
-// FP64 / MIXED, the split-TF32 tensor-core kernels in MIXED_TC.
+// FP64 launches when the blocks are small (below; in every precision form: for blocks this small
+// a tensor-core GEMM pipeline per k-point is mostly fixed cost), else per k-point: cuBLAS ZGEMMs
+// in FP64 / MIXED, the split-TF32 tensor-core kernels in MIXED_TC.
 //
 // The first call for a given set of arrays and band counts autotunes the launch
 // shape (slab chunk size, kernel B band grouping, split count of the tensor-core
@@ -85,7 +86,7 @@ struct Call {
   int total = 0;
 };
 
-// Projector products of every k-point of the batch at once (FP64 / MIXED), for blocks of at
+// Projector products of every k-point of the batch at once (FP64, every precision form), for blocks of at
 // most kNlMax projectors and kNlMax bands per k-point. Per k-point ZGEMMs of a few dozen
 // projectors and bands are latency-bound launches (two per k-point, one after the other); here
 //   k_batch_proj:   partial P_k = X_k^H psi_k over a slice of plane waves, per (k, slice)
@@ -441,7 +442,7 @@ int cpw_b200_kbatch_hk_psi_device(cpw_b200_kbatch* b, const int* nb, void* const
     // CPW_B200_KBATCH_NL=0 keeps one ZGEMM pair per k-point
     {
       const char* v = getenv("CPW_B200_KBATCH_NL");
-      bool small = b->precision != 2 && !(v && atoi(v) == 0);
+      bool small = !(v && atoi(v) == 0);
       std::vector<NlDesc> nd(b->nk);
       long long poff = 0;
       int mmax = 0;
