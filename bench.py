@@ -278,7 +278,7 @@ def run_eig_study(args, local):
         torch.cuda.synchronize()
         icmax = args.icmax_ref if (name == "fp64" and args.icmax_ref) else args.icmax
         r = E.eigensolve(ctx, P, HP, nb, d["mtxds"], d["hamsm"], d["hdiag"], epspsi=args.epspsi, icmax=icmax,
-                         trace=True)
+                         trace=True, ipr=args.ipr)
         ctx.close()
         traces[name] = r["trace"]
         if args.save_traces:
@@ -566,6 +566,7 @@ def main():
                     "(fp64 always runs first as the reference)")
     ap.add_argument("--icmax-ref", type=int, default=0, help="eig mode: outer iterations of the FP64 reference run "
                     "(default: --icmax)")
+    ap.add_argument("--ipr", type=int, default=0, help="eig mode: eigensolver print level (2: phase timers)")
     ap.add_argument("--save-traces", default="", help="eig mode: directory for the iteration traces (.npy)")
     ap.add_argument("--bands", type=int, default=NB, help="profile mode: bands per call")
     ap.add_argument("--precision", choices=["fp64", "mixed", "mixed_tc"], default="fp64", help="profile mode precision")

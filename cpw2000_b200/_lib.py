@@ -29,6 +29,8 @@ SIGNATURES = {
     "cpw_b200_synchronize": (I, [P]),
     "cpw_b200_set_precision": (I, [P, I]),
     "cpw_b200_set_slab_budget": (I, [P, LL]),
+    "cpw_b200_set_wait_limits": (I, [P, LL, LL]),
+    "cpw_b200_wait_selftest": (I, [P, LL, P]),
     "cpw_b200_timing_begin": (I, [P]),
     "cpw_b200_timing_end": (I, [P, DP, C.POINTER(C.c_longlong), I]),
     "cpw_b200_set_kpoint": (I, [P, I, IP, IP, I, DP, IP]),

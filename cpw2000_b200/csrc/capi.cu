@@ -3,7 +3,9 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <atomic>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -217,13 +219,95 @@ void dropin_abandon(cpw_b200_ctx* c) {
   if (c->s_in) cudaStreamSynchronize(c->s_in);
 }
 
+// ---- host-side content checks of the drop-in's inputs ----
+// The drop-in keeps host shadows of what it uploaded and compares the caller's arrays with them
+// on every call. The projectors of a large cell are over a gigabyte (Si216: 88,951 x 864 complex),
+// so the compare and the shadow copy are split over host threads; in hk_psi_c16 the compare runs
+// while the device already computes with the previous call's arrays.
+unsigned host_threads(size_t bytes) {
+  unsigned nt = std::thread::hardware_concurrency();
+  if (nt == 0) nt = 1;
+  const size_t by_size = std::max<size_t>(1, bytes >> 23);     // at least 8 MB per thread
+  return (unsigned)std::min<size_t>(std::min<size_t>(nt, 32), by_size);
+}
+
+// runs f(c0, c1) over [0, n) split into contiguous ranges, one per thread
+template <class F> void par_ranges(size_t n, unsigned nt, F f) {
+  nt = (unsigned)std::max<size_t>(1, std::min<size_t>(nt, n));
+  if (nt <= 1) {
+    f((size_t)0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  th.reserve(nt);
+  for (unsigned t = 0; t < nt; ++t) th.emplace_back(f, n * t / nt, n * (t + 1) / nt);
+  for (auto& x : th) x.join();
+}
+
+// true when ncol columns of `rows` doubles at h (leading dimension ld doubles) equal the packed shadow
+bool cols_equal(const std::vector<double>& sh, const double* h, size_t rows, size_t ld, size_t ncol) {
+  if (sh.size() != rows * ncol) return false;
+  if (rows == 0 || ncol == 0) return true;
+  std::atomic<bool> diff(false);
+  const unsigned nt = host_threads(rows * ncol * 8);
+  if (ld == rows || ncol < nt) {
+    // one contiguous run per column (or a single flat run): split the bytes of each column
+    for (size_t j = 0; j < ncol && !diff.load(std::memory_order_relaxed); ++j) {
+      const double* a = sh.data() + j * rows;
+      const double* b = h + j * ld;
+      const size_t n = (ld == rows) ? rows * ncol : rows;
+      par_ranges(n, host_threads(n * 8), [&](size_t i0, size_t i1) {
+        if (memcmp(a + i0, b + i0, (i1 - i0) * 8)) diff = true;
+      });
+      if (ld == rows) break;
+    }
+  } else {
+    par_ranges(ncol, nt, [&](size_t c0, size_t c1) {
+      for (size_t j = c0; j < c1 && !diff.load(std::memory_order_relaxed); ++j)
+        if (memcmp(sh.data() + j * rows, h + j * ld, rows * 8)) diff = true;
+    });
+  }
+  return !diff.load();
+}
+
+void cols_copy(std::vector<double>& sh, const double* h, size_t rows, size_t ld, size_t ncol) {
+  sh.resize(rows * ncol);
+  if (rows == 0 || ncol == 0) return;
+  par_ranges(ncol, host_threads(rows * ncol * 8), [&](size_t c0, size_t c1) {
+    for (size_t j = c0; j < c1; ++j) memcpy(sh.data() + j * rows, h + j * ld, rows * 8);
+  });
+}
+
+// the caller's projectors equal the ones on the device (compared with the host shadows)
+bool dropin_proj_same(cpw_b200_ctx* c, const double* anlga, const double* xnlkb, int nanl, int mxddim) {
+  if (c->sh_nanl != nanl) return false;
+  if (nanl == 0) return true;
+  if (!same(c->sh_xnl, xnlkb, (size_t)nanl)) return false;
+  return cols_equal(c->sh_anl, anlga, 2 * (size_t)c->mtxd, 2 * (size_t)mxddim, (size_t)nanl);
+}
+
+int dropin_proj_upload(cpw_b200_ctx* c, const double* anlga, const double* xnlkb, int nanl, int mxddim) {
+  if (int s = ctx_set_projectors(c, nanl, anlga, mxddim, xnlkb, false)) {
+    c->sh_nanl = -1;
+    return s;
+  }
+  c->sh_nanl = nanl;
+  c->sh_xnl.assign(xnlkb, xnlkb + nanl);
+  cols_copy(c->sh_anl, anlga, 2 * (size_t)c->mtxd, 2 * (size_t)mxddim, (size_t)nanl);
+  return kOk;
+}
+
 // Bring the default context in line with the k-point arguments of a drop-in call: the
 // k-point arrays are compared with the previous call's shadows and re-uploaded only when
-// they changed; the projectors when lnewanl is set, the basis changed or nanl changed (then
-// lnewanl is cleared). The potential is the caller's next step (sync_dropin_potential).
+// they changed. The projectors are uploaded at once when lnewanl is set (the reference's
+// "anlga recalculated" hint, hk_psi_c16.f90:74; the library only reads it), the basis changed
+// or nanl changed; otherwise they are compared by content, now (defer false) or, with defer,
+// by the caller while the device computes (*pending then tells it to). The potential is the
+// caller's next step (sync_dropin_potential).
 int sync_dropin_kpoint(cpw_b200_ctx* c, int m, int ng, const int* kgv, const double* ekpg, const int* isort,
                        const int* kmscr, const double* anlga, const double* xnlkb, int nanl, int mxddim,
-                       int* lnewanl) {
+                       bool lnewanl, bool defer, bool* pending) {
+  *pending = false;
   std::vector<int> kg((size_t)3 * m);
   for (int i = 0; i < m; ++i) {
     const int it = isort[i];
@@ -238,6 +322,8 @@ int sync_dropin_kpoint(cpw_b200_ctx* c, int m, int ng, const int* kgv, const dou
     // the compact kgv(3, mtxd) of the basis with isort = 1..mtxd is what the device needs
     std::vector<int> iota(m);
     for (int i = 0; i < m; ++i) iota[i] = i + 1;
+    c->sh_mtxd = -1;
+    c->sh_nanl = -1;
     if ((s = ctx_set_basis(c, m, iota.data(), kg.data(), m, ekpg, kmscr))) return s;
     c->sh_mtxd = m;
     c->sh_kmscr.assign(kmscr, kmscr + 7);
@@ -246,10 +332,12 @@ int sync_dropin_kpoint(cpw_b200_ctx* c, int m, int ng, const int* kgv, const dou
     c->sh_ekpg.assign(ekpg, ekpg + m);
     c->sh_vscr.clear();
   }
-  if (kchanged || *lnewanl != 0 || c->nanl != nanl) {
-    if ((s = ctx_set_projectors(c, nanl, anlga, mxddim, xnlkb, false))) return s;
-    *lnewanl = 0;
+  if (kchanged || lnewanl || c->sh_nanl != nanl) return dropin_proj_upload(c, anlga, xnlkb, nanl, mxddim);
+  if (defer) {
+    *pending = true;
+    return kOk;
   }
+  if (!dropin_proj_same(c, anlga, xnlkb, nanl, mxddim)) return dropin_proj_upload(c, anlga, xnlkb, nanl, mxddim);
   return kOk;
 }
 
@@ -350,6 +438,20 @@ int cpw_b200_set_slab_budget(cpw_b200_ctx* c, long long bytes) {
   if (bytes <= 0) return fail(kBadArg, "set_slab_budget: bytes must be positive");
   c->slab_budget = (size_t)bytes;
   return kOk;
+}
+
+int cpw_b200_set_wait_limits(cpw_b200_ctx* c, long long mbarrier_ns, long long grid_polls) {
+  if (int s = check_ctx(c)) return s;
+  c->tcs.wait_ns = mbarrier_ns < 0 ? 2000000000ull : (unsigned long long)mbarrier_ns;
+  c->grid_polls = grid_polls < 0 ? (1LL << 24) : grid_polls;
+  return kOk;
+}
+
+int cpw_b200_wait_selftest(cpw_b200_ctx* c, long long limit_ns, void* stream) {
+  if (int s = check_ctx(c)) return s;
+  if (limit_ns < 0 || limit_ns > 2000000000LL) return fail(kBadArg, "wait_selftest: limit outside 0 .. 2 s");
+  cudaSetDevice(c->device);
+  return tc_wait_selftest(c, (unsigned long long)limit_ns, stream ? (cudaStream_t)stream : c->stream);
 }
 
 int cpw_b200_timing_begin(cpw_b200_ctx* c) {
@@ -537,29 +639,38 @@ int cpw_b200_hk_psi_c16(const int* mtxd, const int* neig, const double* psi, dou
       return s;
     }
   }
-  if ((s = sync_dropin_kpoint(c, m, *ng, kgv, ekpg, isort, kmscr, anlga, xnlkb, *nanl, *mxddim, lnewanl))) {
+  // lnewanl is only read: a caller may pass a literal (berry_derivative.f90:229 passes .TRUE.)
+  bool proj_pending = false;
+  if ((s = sync_dropin_kpoint(c, m, *ng, kgv, ekpg, isort, kmscr, anlga, xnlkb, *nanl, *mxddim, *lnewanl != 0, go,
+                              &proj_pending))) {
     dropin_abandon(c);
     return s;
   }
   bool uploaded = false;
-  if (!go || !c->have_pot) {
+  const bool pot_pending = go && c->have_pot;
+  if (!pot_pending) {
     if ((s = sync_dropin_potential(c, vscr, kmscr, *mxdscr, &uploaded))) {
       dropin_abandon(c);
       return s;
     }
-    return go ? dropin_compute_out(c, pipe, hpsi) : kOk;
   }
-  // the potential on the device is the previous call's: compute with it while vscr is
-  // compared on the host (it changes only between SCF iterations); if it changed, upload
-  // it and compute again from the wavefunctions already on the device
+  if (!go) return kOk;
+  if (!pot_pending && !proj_pending) return dropin_compute_out(c, pipe, hpsi);
+  // the potential and the projectors on the device are the previous call's: compute with them
+  // while vscr and anlga/xnlkb are compared on the host (an SCF changes vscr only between
+  // iterations, the projectors only with the k-point); if either changed, upload it and compute
+  // again from the wavefunctions already on the device
   if ((s = dropin_compute_out(c, pipe, hpsi, false))) {
     dropin_wait(c);
     return s;
   }
   const size_t nv = (size_t)kmscr[6] * kmscr[4] * kmscr[5];
-  if (same(c->sh_vscr, vscr, nv)) return dropin_wait(c);
+  const bool vsame = !pot_pending || cols_equal(c->sh_vscr, vscr, nv, nv, 1);
+  const bool psame = !proj_pending || dropin_proj_same(c, anlga, xnlkb, *nanl, *mxddim);
+  if (vsame && psame) return dropin_wait(c);
   if ((s = dropin_wait(c))) return s;
-  if ((s = sync_dropin_potential(c, vscr, kmscr, *mxdscr, &uploaded))) return s;
+  if (!vsame && (s = sync_dropin_potential(c, vscr, kmscr, *mxdscr, &uploaded))) return s;
+  if (!psame && (s = dropin_proj_upload(c, anlga, xnlkb, *nanl, *mxddim))) return s;
   return dropin_compute_out(c, pipe, hpsi);
 }
 
@@ -573,11 +684,12 @@ void hk_psi_c16_(const int* mtxd, const int* neig, const double* psi, double* hp
 }
 
 namespace {
-// the spinor drop-in keeps its own context and host shadows of its k-point and potential
+// the spinor drop-in keeps its own context and host shadows of its k-point, potential and
+// projectors (compared by content on every call, like the scalar drop-in's)
 struct SpinDropin {
   cpw_b200_ctx* c = nullptr;
   std::vector<int> isort, kgv, kmscr;
-  std::vector<double> ekpg, vscr;
+  std::vector<double> ekpg, vscr, anl, xnl;
   int nanl = -1;
 };
 SpinDropin g_spin;
@@ -635,10 +747,15 @@ int cpw_b200_hk_psi_spin_c16(const int* mtxd, const int* neig, const double* psi
     if ((s = ctx_set_potential_spin(c, vscr_sp, *mxdscr, *nsp))) return s;
     d.vscr.assign(vscr_sp, vscr_sp + nv);
   }
-  if (new_basis || *lnewanl || d.nanl != *nanlsp) {
+  // lnewanl (only read) forces the upload; otherwise the spinor projectors are compared by content
+  const size_t prow = 4 * (size_t)m, pld = 4 * (size_t)*mxddim;    // doubles per column: 2 mtxd complex rows
+  if (new_basis || *lnewanl != 0 || d.nanl != *nanlsp || !same(d.xnl, xnlkbsp, (size_t)*nanlsp) ||
+      !cols_equal(d.anl, anlsp, prow, pld, (size_t)*nanlsp)) {
+    d.nanl = -1;
     if ((s = ctx_set_projectors_spin(c, *nanlsp, anlsp, 2LL * *mxddim, xnlkbsp))) return s;
     d.nanl = *nanlsp;
-    *lnewanl = 0;
+    d.xnl.assign(xnlkbsp, xnlkbsp + *nanlsp);
+    cols_copy(d.anl, anlsp, prow, pld, (size_t)*nanlsp);
   }
   if (m == 0 || nb == 0) return kOk;
   const size_t rows = 2 * (size_t)m;
@@ -700,7 +817,9 @@ int cpw_b200_ditsp_c16(const int* ipr, int* ifail, const int* icmax, const int* 
   const int m = *mtxd, nb = *mxdbnd;
   int s;
   bool uploaded = false;
-  if ((s = sync_dropin_kpoint(c, m, *ng, kgv, ekpg, isort, kmscr, anlga, xnlkb, *nanl, *mxddim, lnewanl)) ||
+  bool proj_pending = false;
+  if ((s = sync_dropin_kpoint(c, m, *ng, kgv, ekpg, isort, kmscr, anlga, xnlkb, *nanl, *mxddim, *lnewanl != 0, false,
+                              &proj_pending)) ||
       (s = sync_dropin_potential(c, vscr, kmscr, *mxdscr, &uploaded)))
     return s;
   const size_t bytes = (size_t)m * nb * 16;
@@ -774,12 +893,9 @@ int cpw_b200_hk_psi_nl_c16(const int* mtxd, const int* neig, const double* psi, 
   cudaSetDevice(c->device);
   DevBuf x, xd, p, h, v;
   int s;
-  if (na == 0) {
-    if (*ladd == 0) {
-      for (int n = 0; n < nb; ++n) memset(hpsi + 2 * (size_t)n * *mxddim, 0, (size_t)m * 16);
-    }
-    return kOk;
-  }
+  // no projectors: the reference skips both products (the `if(nanl > 0)` of
+  // hk_psi_nl_c16.f90:78-98), so hpsi is left as it is even when ladd is false
+  if (na == 0) return kOk;
   if ((s = h.ensure((size_t)m * nb * 16)) || (s = x.ensure((size_t)m * na * 16)) || (s = p.ensure((size_t)na * nb * 16)) ||
       (s = v.ensure((size_t)m * nb * 16)) || (s = xd.ensure((size_t)na * 8)))
     return s;

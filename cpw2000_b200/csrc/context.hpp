@@ -71,7 +71,9 @@ int ctx_pot_local(cpw_b200_ctx* c, int n1, int n2, int n3, int id, int ng, const
 // per-call scratch of the tensor-core projector products and their sticky error flag
 struct TcScratch {
   DevBuf b1, part, b2, err;
+  unsigned long long wait_ns = 2000000000ull;   // hand-off wait limit of the tensor-core GEMMs
 };
+int tc_wait_selftest(cpw_b200_ctx* c, unsigned long long limit_ns, cudaStream_t st);
 int tc_error_flag(TcScratch& t);
 int tc_read_error(TcScratch& t);
 int tc_prepare_projectors(cpw_b200_ctx* c);
@@ -142,6 +144,8 @@ struct cpw_b200_ctx {
   int nanl_sp = 0;
   cpwb::DevBuf anl_sp, anld_sp, sp_idx2, sp_ek2;
 
+  // poll limit of the eigensolver's cooperative grid barrier (bounded device wait)
+  long long grid_polls = 1LL << 24;
   // eigensolver device buffers and cuSOLVER handle, kept between calls (ditsp.cu)
   cpwb::DevBuf ditsp_pool[20];
   void* ditsp_sol = nullptr;
@@ -151,10 +155,11 @@ struct cpw_b200_ctx {
   // slab for the band chunk and staging for host-array entry points
   cpwb::DevBuf slab, h_in, h_out;
 
-  // host shadows used by the drop-in to decide what to re-upload
+  // host shadows used by the drop-in to decide what to re-upload (the projectors are compared by
+  // content: the reference recomputes anlga without any obligation to raise lnewanl)
   std::vector<int> sh_isort, sh_kgv, sh_kmscr;
-  std::vector<double> sh_ekpg, sh_vscr;
-  int sh_mtxd = -1;
+  std::vector<double> sh_ekpg, sh_vscr, sh_anl, sh_xnl;
+  int sh_mtxd = -1, sh_nanl = -1;
 };
 
 namespace cpwb {

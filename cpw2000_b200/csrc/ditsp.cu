@@ -134,13 +134,12 @@ struct MgsArgs {
   unsigned* bar;        // [0] arrival count, [1] generation
   int* err;             // set to 1 when a barrier wait gives up
   double eps, peq, rep; // 1e-20 (as compiled), tiny/eps, 0.9999
+  long long spin_limit; // polls of a grid-barrier wait before it gives up (2^24: ~1 s at ~64 ns per try)
 };
-
-constexpr long long kBarrierSpinLimit = 1LL << 24;   // ~1 s at ~64 ns per try
 
 // Grid barrier with a bounded wait: returns false (and sets *err) if the
 // other CTAs did not arrive in time; all CTAs then leave the kernel.
-__device__ bool grid_barrier(unsigned* bar, int* err) {
+__device__ bool grid_barrier(unsigned* bar, int* err, long long spin_limit) {
   __syncthreads();
   __shared__ int ok;
   if (threadIdx.x == 0) {
@@ -155,7 +154,7 @@ __device__ bool grid_barrier(unsigned* bar, int* err) {
     } else {
       long long it = 0;
       while (*vgen == g) {
-        if (++it > kBarrierSpinLimit) {
+        if (++it > spin_limit) {
           atomicExch(err, 1);
           ok = 0;
           break;
@@ -178,7 +177,7 @@ __device__ bool grid_sum(const MgsArgs& a, int& round, const double* v, int k, d
     if (threadIdx.x == 0) buf[(size_t)blockIdx.x * 4 + t] = s;
   }
   ++round;
-  if (!grid_barrier(a.bar, a.err)) return false;
+  if (!grid_barrier(a.bar, a.err, a.spin_limit)) return false;
   for (int t = 0; t < k; ++t) {
     double s = 0.0;
     for (unsigned b = 0; b < gridDim.x; ++b) s += ((volatile double*)buf)[(size_t)b * 4 + t];
@@ -597,6 +596,7 @@ struct Solver {
     a.eps = CEPS20;
     a.peq = (1.0 / CEPS20) * 2.2250738585072014e-308;
     a.rep = C0P9999;
+    a.spin_limit = c->grid_polls;
     void* args[] = {&a};
     if ((s = ck(cudaLaunchCooperativeKernel((const void*)k_mgs, dim3(grid), dim3(256), args, 0, st), "mgs launch")))
       return s;

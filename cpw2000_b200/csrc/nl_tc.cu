@@ -87,6 +87,7 @@ struct GemmArgs {
   double* out;                 // mode 0: out[split][n][M]; mode 1: complex128 hpsi, ld ldh
   long long ldh;
   int* err;
+  unsigned long long wait_ns;  // limit of the hand-off waits between the roles
 };
 
 struct Item {
@@ -174,14 +175,18 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
   return t;
 }
 
-// wait bounded in time; gives up early once another role has recorded a failure
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, const volatile int* failed) {
+// wait bounded in time (limit_ns); gives up early once another role has recorded a failure.
+// The hand-offs between the roles use the caller's limit (GemmArgs::wait_ns, 2 s unless a
+// failure-detection test shortens it); the waits for copies and MMAs already issued, before the
+// CTA exits, always use kWaitNs: those complete on their own.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, const volatile int* failed,
+                                          unsigned long long limit_ns = kWaitNs) {
   const unsigned long long t0 = globaltimer_ns();
   for (unsigned it = 0;; ++it) {
     if (mbar_try(mbar, parity)) return true;
     if ((it & 63) == 63) {
       if (failed && *failed) return false;
-      if (globaltimer_ns() - t0 > kWaitNs) return false;
+      if (globaltimer_ns() - t0 > limit_ns) return false;
     }
   }
 }
@@ -287,7 +292,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
           if (i + kPrefetch < w.nblk) prefetch(i + kPrefetch);
           const int s = (int)(gk % kStages);
           const long long r = gk / kStages;
-          if (r > 0 && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((r - 1) & 1), &failed)) {
+          if (r > 0 && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((r - 1) & 1), &failed, g.wait_ns)) {
             failed = 1;
             atomicExch(g.err, 1);
             break;
@@ -317,7 +322,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
         const uint32_t idesc = instr_desc(w.n_mma);
         const int nchunk = (w.nblk + chain - 1) / chain;
         // the previous work item's correction accumulator must have been read
-        if (nit > 0 && !mbar_wait(smem_u32(corre), (uint32_t)((nit - 1) & 1), &failed)) {
+        if (nit > 0 && !mbar_wait(smem_u32(corre), (uint32_t)((nit - 1) & 1), &failed, g.wait_ns)) {
           failed = 1;
           atomicExch(g.err, 1);
           break;
@@ -325,7 +330,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
         for (int q = 0; q < nchunk && !failed; ++q, ++gq) {
           const int b = (int)(gq % kMainBufs);
           if (gq >= kMainBufs &&
-              !mbar_wait(smem_u32(&acce[b]), (uint32_t)((gq / kMainBufs - 1) & 1), &failed)) {
+              !mbar_wait(smem_u32(&acce[b]), (uint32_t)((gq / kMainBufs - 1) & 1), &failed, g.wait_ns)) {
             failed = 1;
             atomicExch(g.err, 1);
             break;
@@ -337,7 +342,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
           bool ok = true;
           for (int i = i0; i < i1; ++i, ++gk) {
             const int s = (int)(gk % kStages);
-            if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((gk / kStages) & 1), &failed)) {
+            if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((gk / kStages) & 1), &failed, g.wait_ns)) {
               ok = false;
               break;
             }
@@ -382,7 +387,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tf32x3(const GemmArgs g) {
       bool ok = true;
       for (int q = 0; q < nchunk; ++q, ++gq) {
         const int b = (int)(gq % kMainBufs);
-        if (!mbar_wait(smem_u32(&accf[b]), (uint32_t)((gq / kMainBufs) & 1), &failed)) {
+        if (!mbar_wait(smem_u32(&accf[b]), (uint32_t)((gq / kMainBufs) & 1), &failed, g.wait_ns)) {
           ok = false;
           failed = 1;
           atomicExch(g.err, 1);
@@ -729,6 +734,7 @@ int tc_nl_apply_ops(TcScratch& t, int m, int na, long long nkb1, long long nkb2,
   g1.terms = terms;
   g1.out = (double*)t.part.p;
   g1.err = (int*)t.err.p;
+  g1.wait_ns = t.wait_ns;
 
   // GEMM 2: mtxd x (2 nb), K = 2 nanl, added into hpsi
   const int mt2 = (m + tc::BM - 1) / tc::BM, nt2 = (2 * nb + tc::BN - 1) / tc::BN;
@@ -750,6 +756,7 @@ int tc_nl_apply_ops(TcScratch& t, int m, int na, long long nkb1, long long nkb2,
   g2.out = (double*)hpsi;
   g2.ldh = ldh;
   g2.err = (int*)t.err.p;
+  g2.wait_ns = t.wait_ns;
 
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(tc::k_gemm_tf32x3<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -822,6 +829,7 @@ int tc_zgemm_nn(cpw_b200_ctx* c, int m, int n, int kk, const void* a, long long 
   g.out = (double*)cm;
   g.ldh = ldc;
   g.err = (int*)c->tcs.err.p;
+  g.wait_ns = c->tcs.wait_ns;
   if ((e = cudaFuncSetAttribute(tc::k_gemm_tf32x3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 tc::kSmemBytes)) != cudaSuccess)
     return cuda_fail(e, "tensor-core GEMM attribute");
@@ -831,5 +839,27 @@ int tc_zgemm_nn(cpw_b200_ctx* c, int m, int n, int kk, const void* a, long long 
 }
 
 int tc_check_error(cpw_b200_ctx* c) { return tc_read_error(c->tcs); }
+
+namespace tc {
+// Failure-detection self-test: one thread waits, through the same bounded wait as the GEMM
+// roles, on an mbarrier that nothing arrives at; when the limit runs out it sets the sticky
+// error flag and the kernel returns.
+__global__ void k_wait_selftest(int* err, unsigned long long limit_ns) {
+  __shared__ alignas(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(smem_u32(&bar), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait(smem_u32(&bar), 0u, nullptr, limit_ns)) atomicExch(err, 1);
+}
+}  // namespace tc
+
+int tc_wait_selftest(cpw_b200_ctx* c, unsigned long long limit_ns, cudaStream_t st) {
+  if (int s = tc_error_flag(c->tcs)) return s;
+  tc::k_wait_selftest<<<1, 32, 0, st>>>((int*)c->tcs.err.p, limit_ns);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? kOk : cuda_fail(e, "wait self-test launch");
+}
 
 }  // namespace cpwb

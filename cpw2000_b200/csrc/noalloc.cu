@@ -1,14 +1,17 @@
 // Allocation-free variant of the local H|psi> (V_loc psi [+ ekpg psi]).
 //
 // Who needs it: callers that cannot call cudaMalloc -- code that runs under a
-// caller-owned memory pool or a fixed device-memory budget, host codes that
+// caller-owned memory pool or a fixed device-memory budget, and host codes that
 // hand this library device buffers they already own and forbid it to grow the
-// device heap, and callers inside regions where an allocation would
-// synchronise the device. Every buffer such a caller passes is its own; the
-// work space this operation needs (the FFT slab of a band chunk, the plane
-// lists of the basis, the twiddle tables and the repacked potential) lives in
-// one file-scope __device__ array of fixed size, so this entry point calls no
+// device heap. Every buffer such a caller passes is its own; the work space
+// this operation needs (the FFT slab of a band chunk, the plane lists of the
+// basis, the twiddle tables and the repacked potential) lives in one
+// file-scope __device__ array of fixed size, so this entry point calls no
 // cudaMalloc, cudaFree or allocating library routine.
+//
+// Each call reads the sphere extent of the basis back to the host (12 bytes)
+// before it sizes the FFT planes, so it returns only after the work queued
+// earlier on its stream and that reduction have finished.
 //
 // The array costs kNoAllocScratchBytes of device memory on every GPU that
 // loads this library, for the life of the process. Every call shares it and
@@ -19,7 +22,8 @@
 //
 // The first call on a device resolves the array's device address with
 // cudaGetSymbolAddress while that device is current; make that first call
-// before any stream capture.
+// before any stream capture. The address is kept for the life of the process:
+// do not use this entry point on a device after cudaDeviceReset.
 #include <stdio.h>
 #include <string.h>
 
@@ -231,7 +235,9 @@ extern "C" int cpw_b200_hk_psi_loc_noalloc(int mtxd, int neig, const void* psi, 
              per_band, room, kNoAllocScratchBytes);
     return fail(kBadArg, buf);
   }
-  const int chunk = (int)std::min<size_t>((size_t)neig, room / per_band);
+  // bands per chunk: what fits in the rest of the array, and at most the 65535 blocks a grid's y
+  // dimension takes (kernels A and C launch one block row per band)
+  const int chunk = (int)std::min<size_t>(std::min<size_t>((size_t)neig, room / per_band), 65535);
 
   // plane lists, twiddles and the repacked potential, all in the scratch array
   k_na_count<<<nblk, 256, 0, st>>>(p, mtxd, kgvb, counts);

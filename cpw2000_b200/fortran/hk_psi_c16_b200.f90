@@ -41,7 +41,7 @@ subroutine hk_psi_c16(mtxd, neig, psi, hpsi, lnewanl,                    &
       import :: c_int, c_double, c_double_complex
       integer(c_int), intent(in) :: mtxd, neig, ng, nanl, mxddim, mxdbnd, mxdanl, mxdgve, mxdscr
       integer(c_int), intent(in) :: kgv(*), isort(*), kmscr(7)
-      integer(c_int), intent(inout) :: lnewanl
+      integer(c_int), intent(in) :: lnewanl
       real(c_double), intent(in) :: ekpg(*), vscr(*), xnlkb(*)
       complex(c_double_complex), intent(in) :: psi(*), anlga(*)
       complex(c_double_complex), intent(inout) :: hpsi(*)
@@ -59,7 +59,7 @@ subroutine hk_psi_c16(mtxd, neig, psi, hpsi, lnewanl,                    &
   if(lnewanl) lnew = 1
   istat = cpw_b200_hk_psi_c16(mtxd, neig, psi, hpsi, lnew, ng, kgv, ekpg, isort,                 &
       vscr, kmscr, anlga, xnlkb, nanl, mxddim, mxdbnd, mxdanl, mxdgve, mxdscr)
-  lnewanl = (lnew /= 0)
+!  lnewanl is never assigned: callers may pass a literal (Src/ALFA/berry_derivative.f90:229)
 
   if(istat /= 0) then
     call c_f_pointer(cpw_b200_last_error(), msg, [512])

@@ -34,9 +34,10 @@ def hk_psi_c16(mtxd, neig, psi, hpsi, lnewanl, ng, kgv, ekpg, isort, vscr, kmscr
     """hpsi(:mtxd, :neig) = H psi, as hk_psi_c16 (psi, hpsi: complex128 (mxddim, mxdbnd)).
 
     ``hpsi`` must be a Fortran-ordered complex128 array; it is written in place
-    and also returned, with the updated ``lnewanl`` (cleared once the library
-    has taken the new projectors). Errors raise ``CpwB200Error`` (the
-    reference stops the program).
+    and also returned, with ``lnewanl`` as the library left it (the library only
+    reads the flag: a set flag forces the projectors to be re-uploaded, and
+    unchanged flags are checked against the projectors' content). Errors raise
+    ``CpwB200Error`` (the reference stops the program).
     """
     L = _lib.lib()
     psi = _as_f(psi, np.complex128)
@@ -111,6 +112,10 @@ class Context:
     def synchronize(self):
         """Wait for the device; raises if a bounded device-side wait gave up."""
         check(self._L.cpw_b200_synchronize(self.handle))
+
+    def set_wait_limits(self, mbarrier_ns: int = -1, grid_polls: int = -1):
+        """Limits of the bounded device waits (negative: the defaults, 2 s and 2^24 polls)."""
+        check(self._L.cpw_b200_set_wait_limits(self.handle, int(mbarrier_ns), int(grid_polls)))
 
     def set_slab_budget(self, nbytes: int):
         check(self._L.cpw_b200_set_slab_budget(self.handle, int(nbytes)))

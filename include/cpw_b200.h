@@ -72,6 +72,23 @@ int cpw_b200_set_precision(cpw_b200_ctx* ctx, int mode);
 /* Device bytes the FFT slab of one band chunk may use (default 512 MiB). */
 int cpw_b200_set_slab_budget(cpw_b200_ctx* ctx, long long bytes);
 
+/* Bounded device waits (failure detection). Every wait of this library's kernels
+ * on another party gives up after a limit, records the failure and lets the
+ * kernel return; the host then reports CPW_B200_TIMEOUT (from
+ * cpw_b200_synchronize for the tensor-core GEMMs, from the eigensolver call for
+ * its cooperative Gram-Schmidt kernel) and the context stays usable.
+ * set_wait_limits: the time limit of the tensor-core GEMMs' hand-off mbarrier
+ *   waits (default 2 s) and the poll limit of the Gram-Schmidt grid barrier
+ *   (default 2^24, ~1 s); a negative value restores the default. The waits for
+ *   copies and tensor-core work already issued, before a kernel exits, keep
+ *   their 2 s limit.
+ * wait_selftest: no counterpart in the reference. Launches one kernel that
+ *   waits, with the GEMMs' bounded wait, on an mbarrier nothing arrives at, for
+ *   at most limit_ns (<= 2 s); the next cpw_b200_synchronize returns
+ *   CPW_B200_TIMEOUT. A test of the failure path that faults no GPU. */
+int cpw_b200_set_wait_limits(cpw_b200_ctx* ctx, long long mbarrier_ns, long long grid_polls);
+int cpw_b200_wait_selftest(cpw_b200_ctx* ctx, long long limit_ns, void* stream);
+
 /* Stage timers (CUDA events around each kernel of a stage, on the stream the
  * kernel runs on). timing_end synchronises and writes per-stage totals in ms
  * and launch counts for stages 0..nstage-1: 0 scatter+inverse xy, 1 inverse z +
@@ -185,10 +202,13 @@ int cpw_b200_stress_inputs_device(cpw_b200_ctx* ctx, int neig, const void* psi, 
 
 /* ---- drop-ins with the reference argument lists ---- */
 
-/* Src/hk_psi/reference/hk_psi_c16.f90:28-32. lnewanl != 0 tells the library
- * that anlga/xnlkb were recomputed; it re-uploads them and sets *lnewanl = 0.
- * The k-point arrays and vscr are compared with the previous call's and
- * re-uploaded only when they changed. */
+/* Src/hk_psi/reference/hk_psi_c16.f90:28-32. lnewanl is only read, never
+ * written (callers pass literals, e.g. Src/ALFA/berry_derivative.f90:229):
+ * lnewanl != 0 makes the library re-upload anlga/xnlkb at once. The k-point
+ * arrays, vscr and anlga/xnlkb are compared by content with the previous
+ * call's (host shadows) and re-uploaded only when they changed; vscr and the
+ * projectors are compared while the device already computes with the
+ * previous call's copies, and a call whose inputs changed computes again. */
 int cpw_b200_hk_psi_c16(const int* mtxd, const int* neig, const double* psi, double* hpsi, int* lnewanl,
                         const int* ng, const int* kgv, const double* ekpg, const int* isort, const double* vscr,
                         const int* kmscr, const double* anlga, const double* xnlkb, const int* nanl,
@@ -204,8 +224,9 @@ void hk_psi_c16_(const int* mtxd, const int* neig, const double* psi, double* hp
  * wave i at row 2i-1 and the down component at row 2i (1-based), vscr_sp
  * real(8)(mxdscr, mxdnsp) with nsp = 1, 2 or 4 columns (1, sigma_z, sigma_x,
  * sigma_y), anlsp complex(8)(2*mxddim, mxdasp) spinor KB projectors. The
- * k-point arrays and vscr_sp are compared with the previous call's; anlsp is
- * re-uploaded when lnewanl != 0 (then cleared), nanlsp or the basis changed. */
+ * k-point arrays, vscr_sp, anlsp and xnlkbsp are compared by content with the
+ * previous call's and re-uploaded when they changed; lnewanl (only read) != 0
+ * forces the projector upload. */
 int cpw_b200_hk_psi_spin_c16(const int* mtxd, const int* neig, const double* psi_sp, double* hpsi_sp,
                              int* lnewanl, const int* ng, const int* kgv, const double* ekpg, const int* isort,
                              const double* vscr_sp, const int* kmscr, const int* nsp, const double* anlsp,
@@ -241,7 +262,8 @@ int cpw_b200_ditsp_device(cpw_b200_ctx* ctx, int ipr, int* ifail, int icmax, int
                           int mxdsml, const double* hdiag, int mxdbnd, long long* ihkpsum, void* stream,
                           double* itlog, int itlog_rows);
 
-/* Src/ditsp/ditsp_c16.f90:20-27 with host arrays (psi, hpsi complex(8) (mxddim, mxdbnd)). */
+/* Src/ditsp/ditsp_c16.f90:20-27 with host arrays (psi, hpsi complex(8) (mxddim, mxdbnd)).
+ * lnewanl is only read, as in cpw_b200_hk_psi_c16 (the projectors are also compared by content). */
 int cpw_b200_ditsp_c16(const int* ipr, int* ifail, const int* icmax, const int* iguess, const double* epspsi,
                        int* lnewanl, int* neig, const int* mtxd, const int* mtxds, double* psi, double* hpsi,
                        double* ei, const double* ekpg, const int* isort, const double* vscr, const int* kmscr,
@@ -295,21 +317,24 @@ int cpw_b200_kbatch_info(cpw_b200_kbatch* b, long long* out, int n);
 /* ---- allocation-free local H|psi> ----
  * No counterpart in the reference. For callers that cannot call cudaMalloc
  * (a caller-owned memory pool or fixed device-memory budget, a host code that
- * owns every device buffer and forbids the library to grow the device heap,
- * or a region where an allocation would synchronise the device):
+ * owns every device buffer and forbids the library to grow the device heap):
  * hpsi = V_loc psi (+ ekpg psi when ekpg is not NULL), the local part of
  * hk_psi_c16, FP64, on `stream` (cudaStream_t; NULL = legacy default stream).
  * Every pointer except kmscr is device memory owned by the caller: psi/hpsi
  * complex128 column-major (ld >= mtxd), kgvb(3, mtxd) = kgv(:, isort(i)) of
- * the basis, ekpg(mtxd) or NULL, vscr(id*n2*n3) in the reference layout;
- * kmscr(7) is host memory. The call allocates nothing: its work space (FFT
+ * the basis, ekpg(mtxd) or NULL, vscr in the reference layout holding at
+ * least kmscr(7)*kmscr(5)*kmscr(6) doubles (id*n2*n3; not checked: a shorter
+ * buffer is read out of bounds); kmscr(7) is host memory. The call allocates nothing: its work space (FFT
  * slab of a band chunk, plane lists, twiddles, repacked potential) is one
  * fixed device array of CPW_B200_NOALLOC_SCRATCH_BYTES held by every GPU that
  * loads the library until the process exits. Sizes whose set-up data or one
  * band's FFT slab do not fit are rejected with CPW_B200_BAD_ARG and a message.
  * All calls share the array: calls that overlap on the GPU race, so serialise
- * them. The first call on a device looks up the array's address with that
- * device current; make it before any stream capture. */
+ * them. Each call reads the sphere extent of the basis back to the host, so
+ * it returns only after the work queued before it on `stream` has finished.
+ * The first call on a device looks up the array's address with that device
+ * current; make it before any stream capture. The address is kept for the
+ * life of the process: do not call this on a device after cudaDeviceReset. */
 #define CPW_B200_NOALLOC_SCRATCH_BYTES (64LL << 20)
 int cpw_b200_hk_psi_loc_noalloc(int mtxd, int neig, const void* psi, long long ldpsi, void* hpsi, long long ldhpsi,
                                 const int* kgvb, const double* ekpg, const double* vscr, const int* kmscr,

@@ -35,10 +35,11 @@ def hk_psi_nl_c16(psi, hpsi, anlga, xnlkb, ladd=True):
 
     dhd = anlga^H psi (:82); dhd(i,:) *= xnlkb(i) (:87-91);
     hpsi = [hpsi if ladd else 0] + anlga dhd (:95).
+    With no projectors (nanl = 0) the reference skips both products, the one
+    that would zero hpsi included (the `if(nanl > 0)` of :78-98): hpsi is
+    returned untouched whatever ladd is.
     """
     if anlga.shape[1] == 0:
-        if not ladd:
-            hpsi[...] = 0
         return hpsi
     dhd = anlga.conj().T @ psi
     dhd *= np.asarray(xnlkb)[:, None]

@@ -132,7 +132,7 @@ def test_dropin_host_arrays_with_leading_dimensions(cuda):
     kgv = np.asfortranarray(d["kgv"])
     out, lnew = H.hk_psi_c16(m, nb, psi, hpsi, True, d["ng"], kgv, d["ekpg"], d["isort"], d["vscr"], d["kmscr"],
                              anl, xnl, d["nanl"], mxddim, mxdbnd, d["nanl"] + 1, d["ng"], d["vscr"].size)
-    assert lnew is False
+    assert lnew is True            # only read by the library
     ref = oracle_hpsi(d, psi[:m], nb)
     assert relerr(hpsi[:m, :nb], ref) < TOL64
     assert np.all(hpsi[m:, :] == 7.0 + 7.0j) and np.all(hpsi[:, nb:] == 7.0 + 7.0j)
@@ -142,6 +142,20 @@ def test_dropin_host_arrays_with_leading_dimensions(cuda):
                  d["nanl"], mxddim, mxdbnd, d["nanl"] + 1, d["ng"], v2.size)
     ref2 = O.hk_psi_c16(m, nb, psi[:m], d["ekpg"], d["isort"], v2, d["kmscr"], d["kgv"], d["anlga"], d["xnlkb"])
     assert relerr(hpsi[:m, :nb], ref2) < TOL64
+    # and so are changed projectors without lnewanl, and a changed xnlkb alone
+    anl2 = np.asfortranarray(anl * (0.75 - 0.25j))
+    H.hk_psi_c16(m, nb, psi, hpsi, False, d["ng"], kgv, d["ekpg"], d["isort"], v2, d["kmscr"], anl2, xnl,
+                 d["nanl"], mxddim, mxdbnd, d["nanl"] + 1, d["ng"], v2.size)
+    ref3 = O.hk_psi_c16(m, nb, psi[:m], d["ekpg"], d["isort"], v2, d["kmscr"], d["kgv"], anl2[:m, : d["nanl"]],
+                        d["xnlkb"])
+    assert relerr(hpsi[:m, :nb], ref3) < TOL64
+    xnl2 = xnl.copy()
+    xnl2[0] = -xnl2[0]
+    H.hk_psi_c16(m, nb, psi, hpsi, False, d["ng"], kgv, d["ekpg"], d["isort"], v2, d["kmscr"], anl2, xnl2,
+                 d["nanl"], mxddim, mxdbnd, d["nanl"] + 1, d["ng"], v2.size)
+    ref4 = O.hk_psi_c16(m, nb, psi[:m], d["ekpg"], d["isort"], v2, d["kmscr"], d["kgv"], anl2[:m, : d["nanl"]],
+                        xnl2[: d["nanl"]])
+    assert relerr(hpsi[:m, :nb], ref4) < TOL64
     # and so is another k-point
     d1 = configs.kpoint_inputs(w, 0)
     m1 = d1["mtxd"]
@@ -165,6 +179,22 @@ def test_dropin_nl_matches_oracle(cuda, ladd):
     H.hk_psi_nl_c16(m, nb, psi, hpsi, d["anlga"], d["xnlkb"], d["nanl"], ladd, m, nb, d["nanl"])
     ref = O.hk_psi_nl_c16(psi, h0.copy(), d["anlga"], d["xnlkb"], ladd=ladd)
     assert relerr(hpsi, ref) < TOL64
+
+
+@pytest.mark.parametrize("ladd", [True, False])
+def test_dropin_nl_without_projectors_leaves_hpsi(cuda, ladd):
+    # nanl = 0: hk_psi_nl_c16.f90:78-98 runs neither product, so hpsi keeps its input values even
+    # when ladd is false (the zeroing lives in the skipped zgemm's beta)
+    w = configs.si2_fcc()
+    d = configs.kpoint_inputs(w, 4)
+    m, nb = d["mtxd"], 3
+    psi = configs.random_psi(m, nb, 8)
+    h0 = configs.random_psi(m, nb, 9)
+    hpsi = np.asfortranarray(h0.copy())
+    H.hk_psi_nl_c16(m, nb, psi, hpsi, np.zeros((m, 0), np.complex128), np.zeros(0), 0, ladd, m, nb, 1)
+    assert np.array_equal(hpsi, h0)
+    ref = O.hk_psi_nl_c16(psi, h0.copy(), np.zeros((m, 0), np.complex128), np.zeros(0), ladd=ladd)
+    assert np.array_equal(ref, h0)
 
 
 def test_wraparound_box_is_rejected(cuda):

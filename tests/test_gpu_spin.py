@@ -90,8 +90,17 @@ def test_dropin_spin_with_leading_dimensions(cuda, nsp):
                                          iptr(kgv), dptr(ekpg), iptr(isort), dptr(vsp), iptr(kmscr), iref(nsp),
                                          zptr(anlp), dptr(xnlp), iref(xnl.size), iref(mxddim), iref(mxdbnd),
                                          iref(mxdasp), iref(d["ng"]), iref(mxdscr), iref(4)))
-        assert lnew.value == 0
+        assert lnew.value == (1 if call == 0 else 0)      # the library never writes lnewanl
         assert relerr(hpsi[:2 * m, :nb], want) < TOL64
+    # projectors changed without the flag: picked up by the content check
+    anlp2 = np.asfortranarray(anlp * 0.5)
+    want2 = oracle(d, psi, nb, vsp, nsp, anl * 0.5, xnl)
+    lnew = C.c_int(0)
+    check(L.cpw_b200_hk_psi_spin_c16(iref(m), iref(nb), zptr(psi), zptr(hpsi), C.byref(lnew), iref(d["ng"]),
+                                     iptr(kgv), dptr(ekpg), iptr(isort), dptr(vsp), iptr(kmscr), iref(nsp),
+                                     zptr(anlp2), dptr(xnlp), iref(xnl.size), iref(mxddim), iref(mxdbnd),
+                                     iref(mxdasp), iref(d["ng"]), iref(mxdscr), iref(4)))
+    assert relerr(hpsi[:2 * m, :nb], want2) < TOL64
 
 
 def test_dropin_spin_rejects_bad_nsp(cuda):
