@@ -1,19 +1,23 @@
-"""Benchmark of the H|psi> drop-in on the Si64 workload (one JSON line on rank 0).
+"""Benchmark of the H|psi> drop-in and the eigensolver on the Si216 workload (one JSON line on rank 0).
 
-Workload (the configuration the headline metric is quoted on): Si 64-atom
-cubic supercell, a = 20.52 bohr, seeded 0.02 bohr displacements, Ecut 16 Ha
-(26,529 plane waves at Gamma), 96^3 FFT box, 256 KB projectors, 160 bands.
-A step is one H|psi> application to all 160 bands (one hk_psi_c16 call).
+Workload (the configuration the headline metric is quoted on): Si 216-atom
+cubic supercell, a = 30.78 bohr, seeded 0.03 bohr displacements, Ecut 16 Ha
+(88,951 plane waves at Gamma), 144^3 FFT box, 864 KB projectors, 480 bands.
+A step is one H|psi> application to all 480 bands at Gamma (one hk_psi_c16 call).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--eig 0|1] [--eig-repeats R] [--eig-kpoints NK]
 
 value: bands/s of the FP64 drop-in with inputs resident in HBM, summed over
-ranks (replicas, one per GPU), device-timed with CUDA events, L2 flushed
-(256 MiB memset) before every timed step. e2e: the same metric through the
-reference-facing C ABI (cpw_b200_hk_psi_c16) on pinned host arrays, the H2D
-copy of psi and the D2H copy of hpsi inside the timed region. --impl reference
-times the CPU restatement of the reference's hk_psi_c16 (C + OpenMP, all host
-threads) on the same workload.
+ranks (replicas, one per GPU), device-timed with CUDA events; psi + hpsi
+(1.37 GB) exceed L2, so no flush between steps. e2e: the same metric through
+the reference-facing C ABI (cpw_b200_hk_psi_c16) on pinned host arrays, the H2D
+copy of psi and the D2H copy of hpsi inside the timed region. time_to_eigvals:
+the eigensolver (ditsp_c16 restated) on Gamma and the 3 random k-points of the
+workload, FP64 drop-in vs the mixed form, to 1e-6 Ha (both) and 1e-8 Ha (FP64),
+median of R repeats, then adjoint forces of both converged sets at Gamma.
+--impl reference times the CPU restatement of the reference's hk_psi_c16
+(C + OpenMP, all host threads) on the same workload, a sample of bands per step.
 """
 from __future__ import annotations
 
@@ -35,15 +39,16 @@ sys.path.insert(0, ROOT)
 from cpw2000_b200 import configs  # noqa: E402
 
 METRIC = "H|psi> bands/s"
-NB = 160
-WORKLOAD = "si64"
+NB = 480
+WORKLOAD = "si216"
+NB64 = 160
 
 
 def workload_desc(d):
-    return {"workload": "si64_cubic_ecut16_box96: Si64 cubic a=20.52, sigma 0.02, Ecut 16 Ha, Gamma, "
-                        f"mtxd {d['mtxd']}, box 96^3, {d['nanl']} KB projectors, {NB} bands",
+    return {"workload": "si216_cubic_ecut16_box144: Si216 cubic a=30.78, sigma 0.03, Ecut 16 Ha, Gamma, "
+                        f"mtxd {d['mtxd']}, box 144^3, {d['nanl']} KB projectors, {NB} bands",
             "bands": NB, "mtxd": int(d["mtxd"]), "box": [int(v) for v in d["kmscr"][3:6]], "nanl": int(d["nanl"]),
-            "l2": "flushed between timed steps (256 MiB memset); psi+hpsi 136 MB > L2 126 MB"}
+            "l2": "not flushed: inputs larger than L2 (psi + hpsi 1.37 GB > 126 MB)"}
 
 
 def measured_peaks():
@@ -120,49 +125,91 @@ def cpu_reference_rate(d, nbands: int, nthreads: int = 0, repeats: int = 1):
     return nbands / min(times), (nthreads or c_ref.max_threads())
 
 
-def time_to_eigvals(d, local, icmax=300, nocc=128):
-    """Eigensolver (ditsp_c16 restated) on the workload, FP64 and mixed, from the start basis.
+def time_to_eigvals(w, inputs, local, repeats=3, workers=4, icmax=400, nocc=None):
+    """Eigensolver (ditsp_c16 restated) on the k-points of the Si216 workload, FP64 drop-in vs mixed.
 
-    Reference values: the FP64 path's Ritz values after icmax outer iterations
-    (that path follows the oracle's trajectory and matches dense truth on the
-    small cells). time-to-eigvals = elapsed time at the first outer iteration
-    whose lowest nocc (occupied) Ritz values are all within the tolerance of
-    the reference values: 1e-8 Ha for FP64, 1e-6 Ha for mixed.
+    Each repeat solves every k-point of ``inputs`` (Gamma + 3 random k) from the start basis
+    (iguess 0, epspsi 1e-5, psi/hpsi with 3*480 columns), ``workers`` k-points in flight on
+    their own contexts (cpw2000_b200.kpoints). Reference values: the FP64 path's converged Ritz
+    values of each k-point (first repeat). Time to eigenvalues of a form at a tolerance = the
+    time from the start of the set until every k-point's lowest nocc (occupied) Ritz values are
+    within the tolerance of the reference values (the latest of the k-points' first such outer
+    iteration). Reported as the median over repeats with the spread, at 1e-6 Ha for both forms
+    and 1e-8 Ha for FP64. Forces: adjoint (Hellmann-Feynman) forces at Gamma from each form's
+    converged occupied wavefunctions; their largest difference in Ha/bohr.
     """
     import torch
 
-    from cpw2000_b200 import ditsp as E
+    from cpw2000_b200 import forces as FF
     from cpw2000_b200 import hk_psi as H
-    dev = torch.device("cuda", local)
-    out = {}
-    traces = {}
-    for name, prec in (("fp64", H.FP64), ("mixed", H.MIXED), ("mixed_tc", H.MIXED_TC)):
-        ctx = H.Context(local, precision=prec).setup(d)
-        ctx.set_slab_budget(4 << 30)
-        P = torch.zeros((3 * NB, d["mtxd"]), dtype=torch.complex128, device=dev).t()
-        HP = torch.zeros_like(P)
-        r = E.eigensolve(ctx, P, HP, NB, d["mtxds"], d["hamsm"], d["hdiag"], epspsi=1e-5, icmax=icmax, trace=True)
-        traces[name] = r["trace"]
-        ctx.close()
-        del P, HP
-    ref = traces["fp64"][-1, 4:4 + NB]
-    for name, tol in (("fp64", 1e-8), ("mixed", 1e-6), ("mixed_tc", 1e-6)):
-        tr = traces[name]
-        err = np.abs(tr[:, 4:4 + nocc] - ref[None, :nocc]).max(axis=1)
-        ok = np.nonzero(err <= tol)[0]
-        k = int(ok[0]) if len(ok) else None
-        out[name] = {"seconds": float(tr[k, 0]) if k is not None else None,
-                     "outer_iterations": k + 1 if k is not None else None,
-                     "hpsi_band_products": int(tr[k, 3]) if k is not None else None,
-                     "tolerance_ha": tol,
-                     "max_err_ha_at_end": float(err[-1]),
-                     "xmax_at_end": float(tr[-1, 1]), "nconv_at_end": int(tr[-1, 2])}
-    for name in ("mixed", "mixed_tc"):
-        if out["fp64"]["seconds"] and out[name]["seconds"]:
-            out[f"speedup_{name}_vs_fp64"] = out["fp64"]["seconds"] / out[name]["seconds"]
-    out["definition"] = (f"lowest {nocc} of {NB} Ritz values within tolerance of the FP64 path's values after "
-                         f"{icmax} outer iterations; epspsi 1e-5; start basis from the {d['mtxds']}x{d['mtxds']} "
-                         "small matrix (iguess 0)")
+    from cpw2000_b200 import kpoints
+    natom = sum(sp.natom for sp in w.species)
+    nocc = nocc or 2 * natom
+    forms = (("fp64", H.FP64), ("mixed_tc", H.MIXED_TC))
+    runs = {name: [] for name, _ in forms}
+    keep = {}
+    for rep in range(repeats):
+        for name, prec in forms:
+            res, secs = kpoints.eigensolve_kpoints(inputs, NB, workers=workers, precision=prec, epspsi=1e-5,
+                                                   icmax=icmax, device=local, mxdbnd=3 * NB, trace=True,
+                                                   keep=nocc if rep == 0 else 0, slab_budget=2 << 30)
+            if rep == 0:
+                keep[name] = res[0].pop("psi")
+                for r in res[1:]:
+                    r.pop("psi", None)
+            runs[name].append((res, secs))
+            torch.cuda.empty_cache()
+    refs = [r["trace"][-1, 4:4 + nocc] for r in runs["fp64"][0][0]]
+
+    def set_time(res, tol):
+        ts, its, hk = [], [], 0
+        for r, ref in zip(res, refs):
+            err = np.abs(r["trace"][:, 4:4 + nocc] - ref[None, :]).max(axis=1)
+            ok = np.nonzero(err <= tol)[0]
+            if not len(ok):
+                return None, None, None
+            ts.append(float(r["trace"][ok[0], 0]))
+            its.append(int(ok[0]) + 1)
+            hk += int(r["trace"][ok[0], 3])
+        return max(ts), its, hk
+
+    out = {"kpoints": [[float(x) for x in w.kpoints[k]] for k in range(len(inputs))],
+           "mtxd": [int(d["mtxd"]) for d in inputs], "occupied": nocc, "repeats": repeats,
+           "kpoints_in_flight": workers}
+    for name, _ in forms:
+        tols = (1e-6, 1e-8) if name == "fp64" else (1e-6,)
+        entry = {}
+        for tol in tols:
+            vals = [set_time(res, tol) for res, _ in runs[name]]
+            times = [v[0] for v in vals if v[0] is not None]
+            key = f"{tol:.0e}".replace("e-0", "e-")
+            entry[f"seconds_to_{key}_ha"] = statistics.median(times) if len(times) == len(vals) else None
+            entry[f"seconds_to_{key}_ha_all"] = [v[0] for v in vals]
+            entry[f"iterations_to_{key}_ha"] = vals[0][1]
+            entry[f"hpsi_band_products_to_{key}_ha"] = vals[0][2]
+        res0 = runs[name][0][0]
+        entry["converged"] = [bool(r["converged"]) for r in res0]
+        entry["outer_iterations"] = [int(r["trace"].shape[0]) for r in res0]
+        entry["set_wall_s"] = [float(sec) for _, sec in runs[name]]
+        entry["max_err_ha_at_end"] = float(max(np.abs(r["trace"][-1, 4:4 + nocc] - ref).max()
+                                               for r, ref in zip(res0, refs)))
+        out[name] = entry
+    a, b = out["fp64"]["seconds_to_1e-6_ha"], out["mixed_tc"]["seconds_to_1e-6_ha"]
+    out["speedup_mixed_tc_vs_fp64_at_1e-6"] = a / b if a and b else None
+    a8 = out["fp64"]["seconds_to_1e-8_ha"]
+    out["speedup_mixed_tc_1e-6_vs_fp64_1e-8"] = a8 / b if a8 and b else None
+    d0 = inputs[0]
+    fc = {}
+    for name in keep:
+        sysm = FF.HFSystem(w, d0, keep[name], np.full(nocc, 2.0), device=local)
+        _, f = FF.forces(sysm)
+        fc[name] = FF.to_cartesian(f, w.adot)
+        sysm.ctx.close()
+    out["force_max_abs_diff_ha_bohr"] = float(np.abs(fc["mixed_tc"] - fc["fp64"]).max())
+    out["force_max_abs_ha_bohr"] = float(np.abs(fc["fp64"]).max())
+    out["definition"] = (f"time from the start of the k-point set until the lowest {nocc} Ritz values of every "
+                         "k-point are within the tolerance of the FP64 path's converged values; epspsi 1e-5; "
+                         "start basis from the small matrix (iguess 0); median over repeats; forces at Gamma")
     return out
 
 
@@ -321,15 +368,20 @@ def run_eig_study(args, local):
     print(json.dumps(out), flush=True)
 
 
+REF_SAMPLE = 24     # bands per step of the CPU arms (of the 480 of the workload)
+
+
 def run_reference(args, rank):
+    """CPU restatement of hk_psi_c16 on the same workload and config as our arm; every step is
+    one call on a sample of REF_SAMPLE bands (the whole 480-band step takes the CPU ~a minute)."""
     if rank != 0:
         return
-    w = configs.si64_cubic()
+    w = configs.si216_cubic()
     d = configs.kpoint_inputs(w, 0)
     from oracle import c_ref
     c_ref.lib()
     nthreads = c_ref.max_threads()
-    sample = 16
+    sample = REF_SAMPLE
     for _ in range(args.warmup):
         cpu_reference_rate(d, sample, nthreads)
     rates = []
@@ -341,12 +393,15 @@ def run_reference(args, rank):
     value = statistics.median(rates)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "bands/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sample / value,
+            "ms_per_full_step_est": 1e3 * NB / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded Gaussian pseudopotentials, random complex128 wavefunctions)",
-            "config": {**workload_desc(d), "sample_bands_per_step": sample},
+            "config": {**workload_desc(d), "parallelism": "single GPU",
+                       "precision": "fp64 drop-in (FP64 pruned FFT, FP64 projector products)"},
             "cpu_baseline": {"value": value, "unit": "bands/s", "cores": nthreads, "kind": "port",
-                             "sample": f"{sample} of {NB} bands per step, C+OpenMP restatement of hk_psi_c16 "
-                                       f"(pruned FFT + ZGEMM loops), {nthreads} threads"},
+                             "sample": f"{sample} of {NB} bands per step (median over steps), C+OpenMP restatement "
+                                       "of hk_psi_c16 (own pruned FFT; projector products as plain loops, like the "
+                                       f"reference built with its vendored netlib BLAS), {nthreads} threads"},
             "e2e": {"value": value, "unit": "bands/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": wall}
     print(json.dumps(line), flush=True)
@@ -367,6 +422,47 @@ def dist_setup(args):
     return world, rank, local, pg
 
 
+def per_band_bytes(d, elem):
+    """Algorithmic bytes per band of the three local kernels (elem: bytes of a complex box value)."""
+    from cpw2000_b200 import crystal
+    kd = crystal.kd_of_basis(d["kgv"], d["isort"])
+    nz = 2 * kd[2] + 1
+    n1, n2, n3 = (int(v) for v in d["kmscr"][3:6])
+    plane = n1 * n2
+    m = d["mtxd"]
+    return {"inv_xy": 16 * m + nz * plane * elem,          # psi in (complex128), kept planes out
+            "z_vloc": 2 * nz * plane * elem,                 # kept planes in and out (+ V once per launch)
+            "fwd_xy": nz * plane * elem + 2 * 16 * m}        # kept planes in, psi in, hpsi out
+
+
+def roofline_of(stages, steps, nb, d, elem, v_bytes, hbm, peak_kind, traffic_per_band=None):
+    """Roofline entry of the dominant local kernel from the live stage timers (CUDA events on the
+    launching stream): algorithmic bytes per launch / average launch duration."""
+    ours = {k: stages[k] for k in ("inv_xy", "z_vloc", "fwd_xy") if stages[k][1]}
+    dom = max(ours, key=lambda k: ours[k][0])
+    tot_ms, launches = ours[dom]
+    bands_per_launch = nb * steps / max(launches, 1)
+    alg = per_band_bytes(d, elem)[dom] * bands_per_launch + (v_bytes if dom == "z_vloc" else 0)
+    avg_s = tot_ms / max(launches, 1) / 1e3
+    achieved = alg / avg_s / 1e9
+    traffic = None
+    if traffic_per_band and dom in traffic_per_band:
+        traffic = traffic_per_band[dom] * bands_per_launch
+    return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic, "alg_bytes_per_launch": alg,
+            "avg_launch_ms": avg_s * 1e3, "bands_per_launch": bands_per_launch}
+
+
+def load_traffic(name):
+    """Per-band DRAM bytes of the local kernels from a committed ncu summary (profiles/), or None."""
+    path = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        tj = json.load(f)
+    return {k: v["bytes_per_band"] for k, v in tj.items() if isinstance(v, dict) and "bytes_per_band" in v}
+
+
 def run_ours(args, world, rank, local, dist):
     import torch
 
@@ -375,8 +471,10 @@ def run_ours(args, world, rank, local, dist):
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    w = configs.si64_cubic()
-    d = configs.kpoint_inputs(w, 0, with_hamsm=True)
+    w = configs.si216_cubic()
+    nk = max(1, min(args.eig_kpoints, len(w.kpoints)))
+    inputs = [configs.kpoint_inputs(w, k, with_hamsm=True) for k in range(nk if args.eig else 1)]
+    d = inputs[0]
     m = d["mtxd"]
     psi_h = configs.random_psi(m, NB, 2024 + rank)
 
@@ -392,18 +490,13 @@ def run_ours(args, world, rank, local, dist):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    psi = torch.from_numpy(np.ascontiguousarray(psi_h.T)).to(dev).t()
-    hpsi = torch.empty((NB, m), dtype=torch.complex128, device=dev).t()
-
-    def timed(ctx, steps, warmup):
+    def timed(ctx, psi, hpsi, steps, warmup):
         for _ in range(warmup):
             ctx.hk_psi(psi, hpsi)
         barrier()
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
         ctx.timing_begin()
         for a, b in evs:
-            flush.zero_()
             a.record()
             ctx.hk_psi(psi, hpsi)
             b.record()
@@ -412,13 +505,16 @@ def run_ours(args, world, rank, local, dist):
         ms = sum(a.elapsed_time(b) for a, b in evs) / steps
         return ms, stages
 
+    hbm, _, peak_kind = measured_peaks()
+    psi = torch.from_numpy(np.ascontiguousarray(psi_h.T)).to(dev).t()
+    hpsi = torch.empty((NB, m), dtype=torch.complex128, device=dev).t()
     results = {}
     sampler = ClockSampler(local)
     sampler.start()
     for prec_name, prec in (("fp64", H.FP64), ("mixed", H.MIXED), ("mixed_tc", H.MIXED_TC)):
         ctx = H.Context(local, precision=prec).setup(d)
-        ctx.set_slab_budget(4 << 30)
-        ms, stages = timed(ctx, args.steps, args.warmup)
+        ctx.set_slab_budget(8 << 30)
+        ms, stages = timed(ctx, psi, hpsi, args.steps, args.warmup)
         ctx.synchronize()
         results[prec_name] = (max_over_ranks(ms), stages)
         ctx.close()
@@ -455,44 +551,32 @@ def run_ours(args, world, rank, local, dist):
     barrier()
     t_e2e = []
     for _ in range(args.steps):
-        flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         dropin(0)
         t_e2e.append(time.perf_counter() - t0)
     barrier()
     e2e_ms = max_over_ranks(1e3 * sum(t_e2e) / len(t_e2e))
+    # the drop-in's result against the device path (same operator, same inputs)
+    ref_dev = torch.empty_like(hpsi)
+    ctx = H.Context(local).setup(d)
+    ctx.set_slab_budget(8 << 30)
+    ctx.hk_psi(psi, ref_dev)
+    ctx.synchronize()
+    ctx.close()
+    got = torch.from_numpy(hpsi_pin.numpy().view(np.complex128).reshape((NB, m))).to(dev).t()
+    e2e_rel = float((got - ref_dev).abs().max() / ref_dev.abs().max())
+    del psi_pin, hpsi_pin, got, ref_dev
 
     ms64, st64 = results["fp64"]
     msmx, stmx = results["mixed"]
     mstc, sttc = results["mixed_tc"]
     value = world * NB / (ms64 / 1e3)
-    hbm, _, peak_kind = measured_peaks()
-    # roofline of the dominant kernel of ours (stage with the largest time share among 0..2)
-    plane = 96 * 96
-    nz = None
-    from cpw2000_b200 import crystal
-    kd = crystal.kd_of_basis(d["kgv"], d["isort"])
-    nz = 2 * kd[2] + 1
-    per_band_bytes = {
-        "inv_xy": 16 * m + nz * plane * 16,
-        "z_vloc": 2 * nz * plane * 16,
-        "fwd_xy": nz * plane * 16 + 2 * 16 * m,
-    }
-    ours = {k: st64[k] for k in ("inv_xy", "z_vloc", "fwd_xy")}
-    dom = max(ours, key=lambda k: ours[k][0])
-    tot_ms, launches = ours[dom]
-    bands_per_launch = NB * args.steps / max(launches, 1)
-    alg = per_band_bytes[dom] * bands_per_launch + (96 ** 3 * 8 if dom == "z_vloc" else 0)
-    avg_launch_s = tot_ms / max(launches, 1) / 1e3
-    achieved = alg / avg_launch_s / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic_si64_fp64.json")
-    if os.path.exists(tpath):
-        with open(tpath) as f:
-            tj = json.load(f)
-        if dom in tj:
-            traffic = tj[dom]["bytes_per_band"] * bands_per_launch
+    n1, n2, n3 = (int(v) for v in d["kmscr"][3:6])
+    roof64 = roofline_of(st64, args.steps, NB, d, 16, n1 * n2 * n3 * 8, hbm, peak_kind,
+                         load_traffic("traffic_si216_fp64.json"))
+    rooftc = roofline_of(sttc, args.steps, NB, d, 8, n1 * n2 * n3 * 4, hbm, peak_kind,
+                         load_traffic("traffic_si216_mixed_tc.json"))
     total_stage_ms = sum(v[0] for v in st64.values())
     line = {
         "metric": METRIC, "value": value, "unit": "bands/s", "n_gpus": world, "steps": args.steps,
@@ -500,13 +584,12 @@ def run_ours(args, world, rank, local, dist):
         "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded Gaussian pseudopotentials, random complex128 wavefunctions)",
         "config": {**workload_desc(d), "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "precision": "fp64 drop-in (FP64 pruned FFT, cuBLAS ZGEMM projectors)"},
+                   "precision": "fp64 drop-in (FP64 pruned FFT, FP64 projector products)"},
         "e2e": {"value": world * NB / (e2e_ms / 1e3), "unit": "bands/s", "h2d_bytes_per_step": 16 * m * NB,
-                "d2h_bytes_per_step": 16 * m * NB,
-                "path": "cpw_b200_hk_psi_c16 (drop-in C ABI) on pinned host arrays"},
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic,
-                     "alg_bytes_per_launch": alg, "avg_launch_ms": avg_launch_s * 1e3},
+                "d2h_bytes_per_step": 16 * m * NB, "ms_per_step": e2e_ms,
+                "path": "cpw_b200_hk_psi_c16 (drop-in C ABI) on pinned host arrays; inputs compared by content "
+                        "on the host every call", "max_rel_diff_vs_device_path": e2e_rel},
+        "roofline": roof64,
         "stages_fp64": {k: {"ms_per_step": v[0] / args.steps, "launches": v[1],
                             "share": v[0] / total_stage_ms if total_stage_ms else None}
                         for k, v in st64.items() if v[1]},
@@ -518,22 +601,59 @@ def run_ours(args, world, rank, local, dist):
                      "speedup_vs_fp64": ms64 / mstc,
                      "precision": "FP32 pruned FFT + V_loc, split-TF32 tcgen05 projector GEMMs "
                                   "(hi.hi + hi.lo + lo.hi, FP64 drain of short FP32 chains)",
-                     "stages": {k: v[0] / args.steps for k, v in sttc.items() if v[1]}},
+                     "stages": {k: v[0] / args.steps for k, v in sttc.items() if v[1]},
+                     "roofline": rooftc},
         "gpu_launches": int(sum(v[1] for k, v in st64.items() if k in ("inv_xy", "z_vloc", "fwd_xy"))),
         "library_launches": {"cublas_zgemm": int(st64["nl_proj"][1] + st64["nl_expand"][1])},
         "clocks": clocks,
     }
+    line["si64"] = si64_throughput(local, max(3, args.steps // 2), 3)
     line["kbatch"] = kbatch_throughput(local, max(3, args.steps // 2), 2)
     if args.eig:
-        line["time_to_eigvals"] = time_to_eigvals(d, local)
-        line["kpoint_eig"] = kpoint_eig(local)
+        line["time_to_eigvals"] = time_to_eigvals(w, inputs, local, repeats=args.eig_repeats,
+                                                  workers=min(args.eig_workers, len(inputs)))
     if rank == 0 and world == 1:
-        rate, cores = cpu_reference_rate(d, 64, repeats=2)
+        rate, cores = cpu_reference_rate(d, REF_SAMPLE, repeats=2)
         line["cpu_baseline"] = {"value": rate, "unit": "bands/s", "cores": cores, "kind": "port",
-                                "sample": "64 of 160 bands, best of 2, C+OpenMP restatement of hk_psi_c16 "
-                                          f"(pruned FFT + ZGEMM loops), {cores} threads"}
+                                "sample": f"{REF_SAMPLE} of {NB} bands, best of 2, C+OpenMP restatement of "
+                                          "hk_psi_c16 (own pruned FFT; projector products as plain loops, like the "
+                                          f"reference built with its vendored netlib BLAS), {cores} threads"}
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def si64_throughput(local, steps, warmup):
+    """H|psi> of the Si64 workload (configs[1]: 26,529 PW, 96^3, 256 projectors, 160 bands): FP64 and
+    MIXED_TC bands/s, device-resident, L2 flushed (256 MiB memset) before each timed step."""
+    import torch
+
+    from cpw2000_b200 import hk_psi as H
+    dev = torch.device("cuda", local)
+    d = configs.kpoint_inputs(configs.si64_cubic(), 0)
+    psi = torch.from_numpy(np.ascontiguousarray(configs.random_psi(d["mtxd"], NB64, 2024).T)).to(dev).t()
+    hpsi = torch.empty_like(psi)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    out = {"workload": f"si64 cubic, Ecut 16 Ha, Gamma, mtxd {d['mtxd']}, 96^3, {d['nanl']} projectors, "
+                       f"{NB64} bands"}
+    for name, prec in (("fp64", H.FP64), ("mixed_tc", H.MIXED_TC)):
+        ctx = H.Context(local, precision=prec).setup(d)
+        ctx.set_slab_budget(4 << 30)
+        for _ in range(warmup):
+            ctx.hk_psi(psi, hpsi)
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            ctx.hk_psi(psi, hpsi)
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        ctx.close()
+        ms = statistics.median(ts)
+        out[name] = {"bands_per_s": NB64 / (ms / 1e3), "ms_per_step": ms}
+    return out
 
 
 def run_profile(args, local):
@@ -575,6 +695,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--eig", type=int, default=1, help="also measure time-to-eigvals (1) or not (0)")
+    ap.add_argument("--eig-repeats", type=int, default=3, help="repeats of the time-to-eigvals sets (median)")
+    ap.add_argument("--eig-kpoints", type=int, default=4, help="k-points of the Si216 workload solved (Gamma first)")
+    ap.add_argument("--eig-workers", type=int, default=4, help="k-points in flight during the eigensolver sets")
     args = ap.parse_args()
     world, rank, local, dist = dist_setup(args)
     try:

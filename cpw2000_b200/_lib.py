@@ -38,6 +38,7 @@ SIGNATURES = {
     "cpw_b200_set_projectors": (I, [P, I, DP, I, DP]),
     "cpw_b200_set_projectors_device": (I, [P, I, P, I, P]),
     "cpw_b200_proj_nl_kb_device": (I, [P, DP, I, IP, DP, I, DP, IP, DP, DP, I, IP, I, DP, P, LL]),
+    "cpw_b200_proj_nl_kb_der_device": (I, [P, I, DP, I, IP, DP, I, DP, IP, DP, DP, I, IP, I, DP, P, LL, LL, P, P]),
     "cpw_b200_pot_local": (I, [P, DP, DP, DP, DP, DP, IP, I, I, IP, DP, DP, I, IP, I, I, I, I]),
     "cpw_b200_hk_psi_kin_device": (I, [P, I, P, LL, P, LL, I, I, P]),
     "cpw_b200_hk_psi_loc_c16_device": (I, [P, I, P, LL, P, LL, I, I, P]),

@@ -520,6 +520,17 @@ int cpw_b200_proj_nl_kb_device(cpw_b200_ctx* c, const double* rkpt, int ntype, c
                         ldanl);
 }
 
+int cpw_b200_proj_nl_kb_der_device(cpw_b200_ctx* c, int nder, const double* rkpt, int ntype, const int* natom,
+                                   const double* rat, int mxdatm, const double* adot, const int* nqnl,
+                                   const double* delqnl, const double* vkb, int mxdlqp, const int* nkb, int nanl,
+                                   double* xnlkb, void* anlga, long long ld, long long mxdanl, void* danlgadrk,
+                                   void* d2anlgadrk2) {
+  if (int s = check_ctx(c)) return s;
+  cudaSetDevice(c->device);
+  return ctx_proj_nl_kb_der(c, nder, rkpt, ntype, natom, rat, mxdatm, adot, nqnl, delqnl, vkb, mxdlqp, nkb, nanl,
+                            xnlkb, anlga, ld, mxdanl, danlgadrk, d2anlgadrk2);
+}
+
 int cpw_b200_pot_local(cpw_b200_ctx* c, double* vscr, double* vmax, double* vmin, double* cmax, const double* veff,
                        int* kmscr, int idshift, int ng, const int* kgv, const double* phase, const double* conj, int ns,
                        const int* inds, int mxdscr, int mxdgve, int mxdnst, int install) {

@@ -86,7 +86,7 @@ int tc_nl_apply(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void*
                 cudaEvent_t t0, cudaEvent_t t1, cudaEvent_t t2);
 int tc_check_error(cpw_b200_ctx* c);
 int tc_zgemm_nn(cpw_b200_ctx* c, int m, int n, int kk, const void* a, long long lda, const void* b, long long ldb,
-                void* cm, long long ldc, cudaStream_t st);
+                void* cm, long long ldc, cudaStream_t st, bool accumulate = false);
 int density_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, const double* occ, void* rho,
                    cudaStream_t st);
 int structure_grad_device(cpw_b200_ctx* c, const void* g, int natom, const int* atom_type, const double* tau,
@@ -147,7 +147,7 @@ struct cpw_b200_ctx {
   // poll limit of the eigensolver's cooperative grid barrier (bounded device wait)
   long long grid_polls = 1LL << 24;
   // eigensolver device buffers and cuSOLVER handle, kept between calls (ditsp.cu)
-  cpwb::DevBuf ditsp_pool[20];
+  cpwb::DevBuf ditsp_pool[24];
   void* ditsp_sol = nullptr;
 
   cpwb::StageTimer timer;
@@ -179,6 +179,10 @@ int ctx_hkpsi_spin_device(cpw_b200_ctx* c, int nb, const void* psi, long long ld
 int ctx_proj_nl_kb(cpw_b200_ctx* c, const double* rkpt, int ntype, const int* natom, const double* rat, int mxdatm,
                    const double* adot, const int* nqnl, const double* delqnl, const double* vkb, int mxdlqp,
                    const int* nkb, int nanl, double* xnlkb_out, void* anlga_out, long long ld_out);
+int ctx_proj_nl_kb_der(cpw_b200_ctx* c, int nder, const double* rkpt, int ntype, const int* natom, const double* rat,
+                       int mxdatm, const double* adot, const int* nqnl, const double* delqnl, const double* vkb,
+                       int mxdlqp, const int* nkb, int nanl, double* xnlkb_out, void* anlga, long long ld,
+                       long long mxdanl, void* danlgadrk, void* d2anlgadrk2);
 int ctx_hkpsi_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh,
                      cudaStream_t st, bool with_kinetic, bool with_nl);
 }  // namespace cpwb

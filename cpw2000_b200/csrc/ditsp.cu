@@ -276,6 +276,21 @@ __global__ void k_patch_gram(Z* G, int k, const int* idx, int nd) {
   }
 }
 
+// out[i] = Re G(i, i): the diagonal of a k x k matrix in one contiguous block (a strided
+// device-to-host copy of 16-byte pieces costs one transfer per element)
+__global__ void k_diag_re(const Z* __restrict__ G, int k, double* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) out[i] = G[(size_t)i * k + i].x;
+}
+
+// zero the strictly upper triangle of a k x k column-major matrix
+__global__ void k_zero_upper(Z* G, int k) {
+  const long long n = (long long)k * k;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(t % k), c = (int)(t / k);
+    if (r < c) G[t] = make_cuDoubleComplex(0.0, 0.0);
+  }
+}
+
 __global__ void k_diag_add(Z* G, int k, double shift) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x)
     G[(size_t)i * k + i].x += shift;
@@ -289,6 +304,9 @@ struct Solver {
   cusolverDnHandle_t sol = nullptr;
   int m;            // mtxd
   int mxdsml, mxdbnd;
+  // The first zcols columns of bas are the small-matrix eigenvectors zero-padded below row zrows = mtxds
+  // (ditsp_c16_start.f90:205-212) and never change: products with them run over zrows rows only.
+  int zcols = 0, zrows = 0;
   long long ldp;    // leading dim of psi/hpsi (device)
   Z* P;             // psi   (ldp x mxdbnd)
   Z* HP;            // hpsi
@@ -300,7 +318,8 @@ struct Solver {
   // inside 1: 3 modified Gram-Schmidt leaves, 4 block passes against the converged vectors
   // outside 0-2: 5 residual norms of the inner loop, 6 span test, 7 relaxation (without H|psi>),
   // 8 Ritz subspace Hamiltonian, 9 Ritz rotations, copies and residual check
-  double tphase[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  // inside 3 (Cholesky QR): 10 Gram products, 11 factorisations with their host reads, 12 triangular solves
+  double tphase[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   long long n_gs = 0, n_gs_vec = 0, n_leaf = 0;
   bool timing = false;
   struct Tick {
@@ -385,8 +404,10 @@ struct Solver {
   }
 
   // Hermitian eigen-decomposition of the n x n device matrix A (ld n) with
-  // zheevd('V','L'): eigenvalues to host w, eigenvectors overwrite A.
-  int diag(Z* A, int n, std::vector<double>& w) {
+  // zheevd('V','L'): eigenvalues to host w, eigenvectors overwrite A. With 0 < nlow < n only the
+  // nlow lowest pairs are computed (zheevdx, range 'I'): w gets nlow values, A their vectors in
+  // its leading nlow columns.
+  int diag(Z* A, int n, std::vector<double>& w, int nlow = 0) {
     w.assign(n, 0.0);
     if (n <= 0) return kOk;
     Tick tk(this, 2);
@@ -394,6 +415,28 @@ struct Solver {
       if (cusolverDnCreate(&sol) != CUSOLVER_STATUS_SUCCESS) return fail(kCusolver, "cusolverDnCreate failed");
     }
     cusolverDnSetStream(sol, st);
+    if (nlow > 0 && nlow < n) {
+      int lw = 0, meig = 0;
+      if (cusolverDnZheevdx_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I, CUBLAS_FILL_MODE_LOWER, n,
+                                       A, n, 0.0, 0.0, 1, nlow, &meig, (double*)eg_d.p,
+                                       &lw) != CUSOLVER_STATUS_SUCCESS)
+        return fail(kCusolver, "zheevdx buffer size");
+      if (int s = work.ensure(sizeof(Z) * (size_t)std::max(lw, 1))) return s;
+      if (int s = info.ensure(sizeof(int))) return s;
+      if (cusolverDnZheevdx(sol, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I, CUBLAS_FILL_MODE_LOWER, n, A, n, 0.0,
+                            0.0, 1, nlow, &meig, (double*)eg_d.p, (Z*)work.p, lw,
+                            (int*)info.p) != CUSOLVER_STATUS_SUCCESS)
+        return fail(kCusolver, "zheevdx");
+      int inf = 0;
+      w.resize(nlow);
+      if (int s = ck(cudaMemcpyAsync(&inf, info.p, sizeof(int), cudaMemcpyDeviceToHost, st), "zheevdx info")) return s;
+      if (int s = ck(cudaMemcpyAsync(w.data(), eg_d.p, sizeof(double) * nlow, cudaMemcpyDeviceToHost, st),
+                     "zheevdx w"))
+        return s;
+      if (int s = ck(cudaStreamSynchronize(st), "zheevdx")) return s;
+      if (inf != 0 || meig != nlow) return fail(kCusolver, "diag_c16 (partial) failed, info = " + std::to_string(inf));
+      return kOk;
+    }
     int lw = 0;
     if (cusolverDnZheevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, A, n,
                                     (double*)eg_d.p, &lw) != CUSOLVER_STATUS_SUCCESS)
@@ -425,9 +468,43 @@ struct Solver {
   DevBuf ham_prev;
   void touch(int c0) { ham_clean = std::max(0, std::min(ham_clean, c0)); }
   bool chol = false;
+  bool partial_eig = false;    // Ritz step: only the eigenpairs its decisions and rotations read
+  long long n_eig_full_again = 0;
   bool tc_rot = false;   // Ritz rotations on the tensor cores (mixed form with tensor-core projectors)
   long long n_chol = 0, n_chol_fallback = 0, n_fb_info = 0, n_fb_drop = 0, n_fb_cond = 0;
-  DevBuf chol_g, chol_work, chol_info, chol_idx;
+  DevBuf chol_g, chol_work, chol_info, chol_idx, chol_diag, chol_tmp, chol_tri;
+  bool chol_gram_gemm = true, chol_apply_gemm = true;
+  // L (lower, k x k in G) -> L^-1 in place, strictly upper part zeroed
+  int chol_inverse(Z* G, int k) {
+    size_t dbytes = 0, hbytes = 0;
+    if (cusolverDnXtrtri_bufferSize(sol, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, k, CUDA_C_64F, G, k, &dbytes,
+                                    &hbytes) != CUSOLVER_STATUS_SUCCESS)
+      return fail(kCusolver, "trtri workspace");
+    std::vector<unsigned char> hwork(std::max<size_t>(hbytes, 1));
+    if (int s = chol_tri.ensure(std::max<size_t>(dbytes, 16))) return s;
+    if (cusolverDnXtrtri(sol, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, k, CUDA_C_64F, G, k, chol_tri.p, dbytes,
+                         hwork.data(), hbytes, (int*)chol_info.p) != CUSOLVER_STATUS_SUCCESS)
+      return fail(kCusolver, "trtri");
+    k_zero_upper<<<std::max(1, std::min(1184, (int)(((long long)k * k + 255) / 256))), 256, 0, st>>>(G, k);
+    int inf = 0;
+    if (int s = ck(cudaMemcpyAsync(&inf, chol_info.p, sizeof(int), cudaMemcpyDeviceToHost, st), "trtri info")) return s;
+    if (int s = ck(cudaStreamSynchronize(st), "trtri")) return s;
+    if (inf != 0) return fail(kCusolver, "cholqr: trtri failed, info = " + std::to_string(inf));
+    return kOk;
+  }
+  // x (m x k) <- x Li^H for the lower-triangular Li stored full (k x k)
+  int apply_right_lh(Z* x, int k, const Z* Li) {
+    if (int s = chol_tmp.ensure(sizeof(Z) * (size_t)m * k)) return s;
+    Z* t = (Z*)chol_tmp.p;
+    if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_C, m, k, k, one, x, m, Li, k, zero, t, m, "cholqr apply")) return s;
+    return ck(cudaMemcpyAsync(x, t, sizeof(Z) * (size_t)m * k, cudaMemcpyDeviceToDevice, st), "cholqr apply");
+  }
+  // the real diagonal of G (k x k) into host h (k doubles)
+  int diag_to_host(const Z* G, int k, double* h) {
+    if (int s = chol_diag.ensure(sizeof(double) * (size_t)k)) return s;
+    k_diag_re<<<std::max(1, std::min(64, (k + 255) / 256)), 256, 0, st>>>(G, k, (double*)chol_diag.p);
+    return ck(cudaMemcpyAsync(h, chol_diag.p, sizeof(double) * (size_t)k, cudaMemcpyDeviceToHost, st), "cholqr diag");
+  }
   long long n_chol_dropped = 0, n_chol_shifted = 0;
   static constexpr double kCholCond = 1e-12;
   int cholqr(bool also, Z* x, Z* hx, int k, int* irow, const double* xscl, bool* fallback) {
@@ -448,7 +525,7 @@ struct Solver {
     if (cusolverDnZpotrf_bufferSize(sol, CUBLAS_FILL_MODE_LOWER, k, G, k, &lw) != CUSOLVER_STATUS_SUCCESS)
       return fail(kCusolver, "zpotrf workspace");
     if ((s = chol_work.ensure(sizeof(Z) * (size_t)std::max(lw, 1)))) return s;
-    std::vector<Z> dg(k), dg0(k);
+    std::vector<double> dg(k), dg0(k);
     std::vector<int> dropped;
     // two plain passes; when the first plain factorisation fails (a nearly dependent block),
     // one shifted pass first (factor G + s I, s = 11 (m k + k (k + 1)) u trace(G), as in the
@@ -457,15 +534,22 @@ struct Solver {
     int done = 0;
     while (done < 2) {
       {
-        const double a1 = 1.0, b0 = 0.0;   // lower triangle of X^H X
-        if (cublasZherk(blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, k, m, &a1, x, m, &b0, G, k) != CUBLAS_STATUS_SUCCESS)
-          return fail(kCublas, "cholqr gram");
+        Tick tg(this, 10);
+        if (chol_gram_gemm) {
+          // X^H X as a full product: cuBLAS's zherk for a block of a few hundred vectors over
+          // ~1e5 rows runs at a fraction of the ZGEMM rate (measured: 6 ms against ~1 ms)
+          if ((s = gemm(CUBLAS_OP_C, CUBLAS_OP_N, k, k, m, one, x, m, x, m, zero, G, k, "cholqr gram")))
+            return s;
+        } else {
+          const double a1 = 1.0, b0 = 0.0;   // lower triangle of X^H X
+          if (cublasZherk(blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, k, m, &a1, x, m, &b0, G, k) !=
+              CUBLAS_STATUS_SUCCESS)
+            return fail(kCublas, "cholqr gram");
+        }
       }
+      Tick tf(this, 11);
       // squared norms of the block's vectors (the Gram diagonal, before the factorisation)
-      if ((s = ck(cudaMemcpy2DAsync(dg0.data(), sizeof(Z), G, sizeof(Z) * (size_t)(k + 1), sizeof(Z), k,
-                                    cudaMemcpyDeviceToHost, st),
-                  "cholqr norms")))
-        return s;
+      if ((s = diag_to_host(G, k, dg0.data()))) return s;
       if (first || shift_now) {
         if ((s = ck(cudaStreamSynchronize(st), "cholqr norms"))) return s;
       }
@@ -474,7 +558,7 @@ struct Solver {
         // the passes against the converged vectors) removes vectors those passes reduced to
         // rounding noise: zero and flag them
         for (int i = 0; i < k; ++i)
-          if (!(dg0[i].x >= CEPS20 * xscl[i]) || !(xscl[i] > 0.0)) dropped.push_back(i);
+          if (!(dg0[i] >= CEPS20 * xscl[i]) || !(xscl[i] > 0.0)) dropped.push_back(i);
         for (int i : dropped) {
           irow[i] = 0;
           if ((s = ck(cudaMemsetAsync(x + (size_t)i * m, 0, sizeof(Z) * m, st), "cholqr drop")) ||
@@ -494,7 +578,7 @@ struct Solver {
             G, k, (const int*)chol_idx.p, (int)dropped.size());
       if (shift_now) {
         double tr = 0.0;
-        for (int i = 0; i < k; ++i) tr += dg0[i].x;
+        for (int i = 0; i < k; ++i) tr += dg0[i];
         const double sh = 11.0 * ((double)m * k + (double)k * (k + 1)) * 1.1102230246251565e-16 * tr;
         k_diag_add<<<std::max(1, std::min(1184, (k + 255) / 256)), 256, 0, st>>>(G, k, sh);
       }
@@ -503,21 +587,18 @@ struct Solver {
         return fail(kCusolver, "zpotrf");
       int info = 0;
       if ((s = ck(cudaMemcpyAsync(&info, chol_info.p, sizeof(int), cudaMemcpyDeviceToHost, st), "cholqr info")) ||
-          (s = ck(cudaMemcpy2DAsync(dg.data(), sizeof(Z), G, sizeof(Z) * (size_t)(k + 1), sizeof(Z), k,
-                                    cudaMemcpyDeviceToHost, st),
-                  "cholqr diag")) ||
-          (s = ck(cudaStreamSynchronize(st), "cholqr")))
+          (s = diag_to_host(G, k, dg.data())) || (s = ck(cudaStreamSynchronize(st), "cholqr")))
         return s;
       first = false;
       bool bad = info != 0;
       int why = bad ? 1 : 0;        // 1 factorisation, 2 drop rule, 3 conditioning
       for (int i = 0; i < k && !bad && done == 0 && !shift_now; ++i) {
         if (irow[i] == 0) continue;
-        const double piv = dg[i].x * dg[i].x;
+        const double piv = dg[i] * dg[i];
         if (!(piv > CEPS20 * xscl[i])) {
           bad = true;
           why = 2;
-        } else if (!(piv > kCholCond * dg0[i].x)) {
+        } else if (!(piv > kCholCond * dg0[i])) {
           bad = true;
           why = 3;
         }
@@ -543,12 +624,21 @@ struct Solver {
         }
         return fail(kCusolver, "cholqr: second Cholesky pass failed");
       }
-      if (cublasZtrsm(blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, CUBLAS_DIAG_NON_UNIT, m, k, &one,
-                      G, k, x, m) != CUBLAS_STATUS_SUCCESS)
-        return fail(kCublas, "cholqr trsm");
-      if (also && cublasZtrsm(blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, CUBLAS_DIAG_NON_UNIT, m,
-                              k, &one, G, k, hx, m) != CUBLAS_STATUS_SUCCESS)
-        return fail(kCublas, "cholqr trsm");
+      tf.stop();
+      Tick tt(this, 12);
+      if (chol_apply_gemm) {
+        // X <- X L^-H as one ZGEMM with the explicit inverse (trtri, then the strictly upper part
+        // zeroed): the triangular solve of a tall block runs far below the ZGEMM rate
+        if ((s = chol_inverse(G, k))) return s;
+        if ((s = apply_right_lh(x, k, G)) || (also && (s = apply_right_lh(hx, k, G)))) return s;
+      } else {
+        if (cublasZtrsm(blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, CUBLAS_DIAG_NON_UNIT, m, k,
+                        &one, G, k, x, m) != CUBLAS_STATUS_SUCCESS)
+          return fail(kCublas, "cholqr trsm");
+        if (also && cublasZtrsm(blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, CUBLAS_DIAG_NON_UNIT, m,
+                                k, &one, G, k, hx, m) != CUBLAS_STATUS_SUCCESS)
+          return fail(kCublas, "cholqr trsm");
+      }
       if (shift_now) {
         shift_now = false;      // the shifted pass conditions the block; two plain passes follow
         continue;
@@ -650,8 +740,10 @@ struct Solver {
     return grsch_mm(also, x + (size_t)nn * m, also ? hx + (size_t)nn * m : nullptr, nn2, irow + nn, xscl + nn);
   }
 
-  // orthonormalise columns [nconv, nvec) of x (ld m) against [0, nconv) twice and among themselves
-  int grsch_loop(bool also, Z* x, Z* hx, int nconv, int nvec, std::vector<int>& irow) {
+  // orthonormalise columns [nconv, nvec) of x (ld m) against [0, nconv) twice and among themselves;
+  // structured: x is bas, whose leading zcols columns vanish below row zrows (hx, when updated, has no
+  // such structure)
+  int grsch_loop(bool also, Z* x, Z* hx, int nconv, int nvec, std::vector<int>& irow, bool structured = false) {
     Tick tk(this, 1);
     irow.assign(std::max(nvec, 0), 1);
     if (nvec <= nconv) return kOk;
@@ -666,13 +758,22 @@ struct Solver {
       Tick tk4(this, 4);
       if (int s = smallA.ensure(sizeof(Z) * (size_t)nconv * k)) return s;
       Z* t = (Z*)smallA.p;
+      // leading columns with zero rows below zrows: their products run over zrows rows
+      const int c0 = structured ? std::min(zcols, nconv) : 0;
+      Z* y = x + (size_t)nconv * m;
       for (int pass = 0; pass < 2; ++pass) {
-        if (int s = gemm(CUBLAS_OP_C, CUBLAS_OP_N, nconv, k, m, one, x, m, x + (size_t)nconv * m, m, zero, t, nconv,
-                         "grsch_loop t"))
+        if (c0 > 0)
+          if (int s = gemm(CUBLAS_OP_C, CUBLAS_OP_N, c0, k, zrows, one, x, m, y, m, zero, t, nconv, "grsch_loop t0"))
+            return s;
+        if (int s = gemm(CUBLAS_OP_C, CUBLAS_OP_N, nconv - c0, k, m, one, x + (size_t)c0 * m, m, y, m, zero, t + c0,
+                         nconv, "grsch_loop t"))
           return s;
-        if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_N, m, k, nconv, mone, x, m, t, nconv, one, x + (size_t)nconv * m, m,
-                         "grsch_loop x"))
+        if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_N, m, k, nconv - c0, mone, x + (size_t)c0 * m, m, t + c0, nconv, one,
+                         y, m, "grsch_loop x"))
           return s;
+        if (c0 > 0)
+          if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_N, zrows, k, c0, mone, x, m, t, nconv, one, y, m, "grsch_loop x0"))
+            return s;
         if (also)
           if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_N, m, k, nconv, mone, hx, m, t, nconv, one, hx + (size_t)nconv * m,
                            m, "grsch_loop hx"))
@@ -738,12 +839,14 @@ struct Solver {
 // would serialise contexts that solve different k-points at the same time.
 struct SolverPool {
   Solver& S;
-  DevBuf* m[20];
+  static constexpr int kN = 23;
+  DevBuf* m[kN];
   explicit SolverPool(Solver& s) : S(s) {
-    DevBuf* l[20] = {&S.bas,  &S.hbas,      &S.smallA,    &S.smallV,   &S.dvec,     &S.dvec2,    &S.dz,
+    DevBuf* l[kN] = {&S.bas,  &S.hbas,      &S.smallA,    &S.smallV,   &S.dvec,     &S.dvec2,    &S.dz,
                      &S.work, &S.info,      &S.eg_d,      &S.hdiag_d,  &S.ham_prev, &S.chol_g,   &S.chol_work,
-                     &S.chol_info, &S.chol_idx, &S.mgs_part, &S.mgs_bar, &S.mgs_irow, &S.mgs_xscl};
-    for (int i = 0; i < 20; ++i) {
+                     &S.chol_info, &S.chol_idx, &S.mgs_part, &S.mgs_bar, &S.mgs_irow, &S.mgs_xscl, &S.chol_diag,
+                     &S.chol_tmp, &S.chol_tri};
+    for (int i = 0; i < kN; ++i) {
       m[i] = l[i];
       swap(*m[i], S.c->ditsp_pool[i]);
     }
@@ -751,7 +854,7 @@ struct SolverPool {
     if (S.sol) cusolverDnSetStream(S.sol, S.st);
   }
   ~SolverPool() {
-    for (int i = 0; i < 20; ++i) swap(*m[i], S.c->ditsp_pool[i]);
+    for (int i = 0; i < kN; ++i) swap(*m[i], S.c->ditsp_pool[i]);
     S.c->ditsp_sol = (void*)S.sol;
     S.sol = nullptr;
   }
@@ -820,6 +923,11 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
   // Cholesky QR twice for the mixed form; CPW_B200_ORTHO=mgs|cholqr overrides
   S.chol = c->precision != 0;
   S.tc_rot = c->precision == 2 && !(getenv("CPW_B200_TC_ROT") && !strcmp(getenv("CPW_B200_TC_ROT"), "0"));
+  // partial subspace eigensolve (zheevdx, lowest pairs only): measured no faster than zheevd on the
+  // Si216 Ritz matrices (~1100), so off unless CPW_B200_EIG_PARTIAL=1
+  S.partial_eig = getenv("CPW_B200_EIG_PARTIAL") && !strcmp(getenv("CPW_B200_EIG_PARTIAL"), "1");
+  S.chol_gram_gemm = !(getenv("CPW_B200_CHOL_GRAM") && !strcmp(getenv("CPW_B200_CHOL_GRAM"), "herk"));
+  S.chol_apply_gemm = !(getenv("CPW_B200_CHOL_APPLY") && !strcmp(getenv("CPW_B200_CHOL_APPLY"), "trsm"));
   if (const char* o = getenv("CPW_B200_ORTHO")) {
     if (!strcmp(o, "mgs")) S.chol = false;
     if (!strcmp(o, "cholqr")) S.chol = true;
@@ -898,6 +1006,10 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
                 "start basis")))
     return s;
   if ((s = S.hk(S.B(0), mtxd, S.HB(0), mtxd, nexact))) return s;
+  if (!(getenv("CPW_B200_ZERO_BLOCKS") && !strcmp(getenv("CPW_B200_ZERO_BLOCKS"), "0"))) {
+    S.zcols = nexact;
+    S.zrows = mtxds;
+  }
   int nitold;
   bool lortho;
   if (iguess != 1) {
@@ -1104,7 +1216,8 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
           S.touch(nexact + nconv);
           if ((s = S.copycols(S.B(nexact + nconv), mtxd, PP + (size_t)nconv * mtxd, mtxd, ntst - nconv))) return s;
           std::vector<int> irowb;
-          if ((s = S.grsch_loop(false, (Z*)S.bas.p, (Z*)S.hbas.p, nexact + nconv, nexact + ntst, irowb))) return s;
+          if ((s = S.grsch_loop(false, (Z*)S.bas.p, (Z*)S.hbas.p, nexact + nconv, nexact + ntst, irowb, true)))
+            return s;
           int ired;
           if ((s = S.grsch_shift((Z*)S.bas.p, mtxd, nexact + nconv, nexact + ntst, irowb, &ired))) return s;
           if (ired > 0) {
@@ -1173,7 +1286,7 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
     {
       std::vector<int> irowb;
       S.touch(nexact + nconv);
-      if ((s = S.grsch_loop(false, (Z*)S.bas.p, (Z*)S.hbas.p, nexact + nconv, nsize, irowb))) return s;
+      if ((s = S.grsch_loop(false, (Z*)S.bas.p, (Z*)S.hbas.p, nexact + nconv, nsize, irowb, true))) return s;
       int ired;
       if ((s = S.grsch_shift((Z*)S.bas.p, mtxd, nexact + nconv, nsize, irowb, &ired))) return s;
       nsize -= ired;
@@ -1198,18 +1311,28 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
                                         sizeof(Z) * (size_t)c, c, cudaMemcpyDeviceToDevice, st),
                       "ritz hamsm reuse")))
           return s;
-        if (c < nsize) {
-          if ((s = S.gemm(CUBLAS_OP_C, CUBLAS_OP_N, nsize - c, c, mtxd, S.one, S.HB(c), mtxd, S.B(0), mtxd, S.zero,
-                          H + c, nsize, "ritz hamsm rows")))
-            return s;
-          if (cublasZherkx(S.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, nsize - c, mtxd, &S.one, S.HB(c), mtxd, S.B(c),
-                           mtxd, &b0, H + (size_t)c * nsize + c, nsize) != CUBLAS_STATUS_SUCCESS)
-            return fail(kCublas, "ritz hamsm");
-        }
       } else {
         ++S.ham_full;
-        if (cublasZherkx(S.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, nsize, mtxd, &S.one, (Z*)S.hbas.p, mtxd,
-                         (Z*)S.bas.p, mtxd, &b0, H, nsize) != CUBLAS_STATUS_SUCCESS)
+      }
+      // rows [c, nsize) of the lower triangle. Columns j < zcols of bas vanish below row zrows, so
+      // hbas(:, i)^H bas(:, j) for those columns runs over zrows rows: one product over zrows rows
+      // for the columns below zcols (the rectangle, upper entries of its diagonal block included, which
+      // zheevd does not read), one over mtxd rows for the columns [zcols, c), and zherkx (the lower
+      // triangle) for the columns [max(c, zcols), nsize).
+      if (c < nsize) {
+        const int cz = std::min(S.zcols, nsize);
+        if (cz > 0 &&
+            (s = S.gemm(CUBLAS_OP_C, CUBLAS_OP_N, nsize - c, cz, S.zrows, S.one, S.HB(c), mtxd, S.B(0), mtxd, S.zero,
+                        H + c, nsize, "ritz hamsm zero-padded columns")))
+          return s;
+        if (c > cz &&
+            (s = S.gemm(CUBLAS_OP_C, CUBLAS_OP_N, nsize - c, c - cz, mtxd, S.one, S.HB(c), mtxd, S.B(cz), mtxd,
+                        S.zero, H + (size_t)cz * nsize + c, nsize, "ritz hamsm rows")))
+            return s;
+        const int d0 = std::max(c, cz);
+        if (d0 < nsize && cublasZherkx(S.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, nsize - d0, mtxd, &S.one,
+                                       S.HB(d0), mtxd, S.B(d0), mtxd, &b0, H + (size_t)d0 * nsize + d0,
+                                       nsize) != CUBLAS_STATUS_SUCCESS)
           return fail(kCublas, "ritz hamsm");
       }
       // keep it for the next Ritz step (zheevd overwrites smallV)
@@ -1220,30 +1343,57 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
       S.ham_prev_n = nsize;
       S.ham_clean = nsize;
     }
+    // The decisions below read the eigenvalues up to the first gap above epsa past ndeg and niter,
+    // and niter is capped at nitcap; psi and hpsi use the first niter eigenvectors. So only the
+    // lowest nitcap + 2 pairs are computed (zheevdx), unless the degeneracy count ndeg runs into
+    // that bound, when the full decomposition is taken (the reference computes all pairs,
+    // ditsp_c16_ritz.f90:200; the decisions are the same).
+    const int nitcap = std::min(std::min((mxdsml - nexact + nconv) / 2, nexact), mxdbnd);
+    int nval = S.partial_eig ? std::min(nsize, nitcap + 2) : nsize;
     std::vector<double> egs;
-    if ((s = S.diag((Z*)S.smallV.p, nsize, egs))) return s;
-    for (int i = 0; i < nsize; ++i) eg[i] = egs[i];
-    ndeg = neig;
-    for (int i = neig; i < nsize; ++i) {
-      if (fabs(eg[i] - eg[i - 1]) > epsa) break;
-      ndeg = i + 1;
+    if (nval < nsize) {
+      // if the full decomposition is needed after all, ham_prev still holds the matrix
+      if ((s = S.diag((Z*)S.smallV.p, nsize, egs, nval))) return s;
+    } else {
+      if ((s = S.diag((Z*)S.smallV.p, nsize, egs))) return s;
     }
+    auto count_ndeg = [&](int nv) {
+      int nd = neig;
+      for (int i = neig; i < nv; ++i) {
+        if (fabs(egs[i] - egs[i - 1]) > epsa) break;
+        nd = i + 1;
+      }
+      return nd;
+    };
+    ndeg = count_ndeg(nval);
+    if (nval < nsize && ndeg == nval) {
+      // a degenerate cluster reaches the computed pairs: decompose fully
+      if ((s = S.ck(cudaMemcpyAsync(S.smallV.p, S.ham_prev.p, sizeof(Z) * (size_t)nsize * nsize,
+                                    cudaMemcpyDeviceToDevice, st),
+                    "ritz hamsm again")))
+        return s;
+      ++S.n_eig_full_again;
+      if ((s = S.diag((Z*)S.smallV.p, nsize, egs))) return s;
+      nval = nsize;
+      ndeg = count_ndeg(nval);
+    }
+    for (int i = 0; i < nsize; ++i) eg[i] = i < nval ? egs[i] : 0.0;
     ndeg = std::min(ndeg, mxdbnd);
     niter = ndeg + 1;
     if (nsize > niter) {
-      for (int i = ndeg + 1; i < nsize; ++i) {
+      for (int i = ndeg + 1; i < nval; ++i) {       // beyond nval niter exceeds nitcap: capped below
         if (fabs(eg[i] - eg[i - 1]) > epsa) break;
         niter = i + 1;
       }
     }
-    {
-      const int nmax = (mxdsml - nexact + nconv) / 2;
-      niter = std::min(std::min(niter, nmax), std::min(nexact, mxdbnd));
-      niter = std::max(niter, ndeg);
-    }
+    niter = std::max(std::min(niter, nitcap), ndeg);
     if (nconv > 0) {
-      std::vector<Z> vh((size_t)nsize * nsize);
-      if ((s = S.ck(cudaMemcpyAsync(vh.data(), S.smallV.p, sizeof(Z) * vh.size(), cudaMemcpyDeviceToHost, st), "vsm")))
+      // the test reads rows [0, nexact + nconv) of the first nconv eigenvectors only
+      const int vrows = std::min(nsize, nexact + nconv);
+      std::vector<Z> vh((size_t)nsize * nconv);
+      if ((s = S.ck(cudaMemcpy2DAsync(vh.data(), sizeof(Z) * (size_t)nsize, S.smallV.p, sizeof(Z) * (size_t)nsize,
+                                      sizeof(Z) * (size_t)vrows, nconv, cudaMemcpyDeviceToHost, st),
+                    "vsm")))
         return s;
       if ((s = S.ck(cudaStreamSynchronize(st), "vsm"))) return s;
       const int kmax = nconv;
@@ -1272,13 +1422,21 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
     // psi = bas V, hpsi = hbas V (ditsp_c16_ritz.f90:284-287): split-TF32 tensor-core products in the
     // mixed form (V and the subspace Hamiltonian stay FP64), FP64 ZGEMM otherwise
     Solver::Tick tk9(&S, 9);
+    // psi: the leading zcols columns of bas vanish below row zrows, so their share of bas V is added
+    // to the first zrows rows only
+    const int cz = std::min(S.zcols, nsize);
+    const Z* V = (const Z*)S.smallV.p;
     if (S.tc_rot) {
-      if ((s = tc_zgemm_nn(c, mtxd, niter, nsize, S.bas.p, mtxd, S.smallV.p, nsize, PP, mtxd, st)) ||
+      if ((s = tc_zgemm_nn(c, mtxd, niter, nsize - cz, S.B(cz), mtxd, V + cz, nsize, PP, mtxd, st)) ||
+          (cz > 0 && (s = tc_zgemm_nn(c, S.zrows, niter, cz, S.bas.p, mtxd, V, nsize, PP, mtxd, st, true))) ||
           (s = tc_zgemm_nn(c, mtxd, niter, nsize, S.hbas.p, mtxd, S.smallV.p, nsize, HPP, mtxd, st)))
         return s;
     } else {
-      if ((s = S.gemm(CUBLAS_OP_N, CUBLAS_OP_N, mtxd, niter, nsize, S.one, (Z*)S.bas.p, mtxd, (Z*)S.smallV.p, nsize,
+      if ((s = S.gemm(CUBLAS_OP_N, CUBLAS_OP_N, mtxd, niter, nsize - cz, S.one, S.B(cz), mtxd, V + cz, nsize,
                       S.zero, PP, mtxd, "ritz psi")))
+        return s;
+      if (cz > 0 && (s = S.gemm(CUBLAS_OP_N, CUBLAS_OP_N, S.zrows, niter, cz, S.one, (Z*)S.bas.p, mtxd, V, nsize, S.one,
+                                PP, mtxd, "ritz psi zero-padded columns")))
         return s;
       if ((s = S.gemm(CUBLAS_OP_N, CUBLAS_OP_N, mtxd, niter, nsize, S.one, (Z*)S.hbas.p, mtxd, (Z*)S.smallV.p, nsize,
                       S.zero, HPP, mtxd, "ritz hpsi")))
@@ -1300,7 +1458,7 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
       row[1] = xmax;
       row[2] = nconv;
       row[3] = (double)S.ihk;
-      for (int i = 0; i < mxdbnd; ++i) row[4 + i] = i < nsize ? eg[i] : 0.0;
+      for (int i = 0; i < mxdbnd; ++i) row[4 + i] = i < std::min(nsize, nval) ? eg[i] : 0.0;
     }
     if (ipr > 2)
       printf("  ditsp_c16_ritz ic = %d  nconv = %d  niter = %d  nsize = %d  ndeg = %d  xmax = %.6e  e1 = %.12f\n", ic,
@@ -1342,6 +1500,9 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
     printf("  ditsp_c16: outside: residual norms %.4f s, span test %.4f s, relaxation %.4f s, Ritz subspace "
            "Hamiltonian %.4f s (%lld reused leading blocks, %lld full), Ritz rotations + residual check %.4f s\n",
            S.tphase[5], S.tphase[6], S.tphase[7], S.tphase[8], S.ham_reused, S.ham_full, S.tphase[9]);
+    printf("  ditsp_c16: Cholesky QR parts: Gram %.4f s, factorisation %.4f s, triangular solves %.4f s; "
+           "partial subspace eigensolves redone in full: %lld\n",
+           S.tphase[10], S.tphase[11], S.tphase[12], S.n_eig_full_again);
     fflush(stdout);
   }
   if ((s = S.ck(cudaStreamSynchronize(st), "ditsp"))) return s;

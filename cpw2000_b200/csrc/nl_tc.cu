@@ -788,14 +788,17 @@ int tc_nl_apply(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void*
                          (const float*)c->tc_a2.p, nb, psi, ldpsi, hpsi, ldh, st, t0, t1, t2);
 }
 
-// C (m x n) = A (m x kk) B (kk x n), complex128 column-major, in split TF32 on the tensor cores
+// C (m x n) = A (m x kk) B (kk x n) (accumulate: C += A B), complex128 column-major, in split TF32
+// on the tensor cores
 int tc_zgemm_nn(cpw_b200_ctx* c, int m, int n, int kk, const void* a, long long lda, const void* b, long long ldb,
-                void* cm, long long ldc, cudaStream_t st) {
+                void* cm, long long ldc, cudaStream_t st, bool accumulate) {
   if (m <= 0 || n <= 0) return kOk;
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  cudaError_t e = cudaMemset2DAsync(cm, sizeof(C2<double>) * (size_t)ldc, 0, sizeof(C2<double>) * (size_t)m, n, st);
+  cudaError_t e = cudaSuccess;
+  if (!accumulate)
+    e = cudaMemset2DAsync(cm, sizeof(C2<double>) * (size_t)ldc, 0, sizeof(C2<double>) * (size_t)m, n, st);
   if (e != cudaSuccess) return cuda_fail(e, "tc zgemm");
   if (kk <= 0) return kOk;
   const long long nkb = (2LL * kk + tc::BK - 1) / tc::BK;

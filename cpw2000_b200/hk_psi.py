@@ -77,6 +77,33 @@ def hk_psi_nl_c16(mtxd, neig, psi, hpsi, anlga, xnlkb, nanl, ladd, mxddim, mxdbn
     return hpsi
 
 
+def _kb_arrays(rkpt, species, vkb, nkb, adot, delq, nq):
+    """The arguments of proj_nl_kb_c16 / proj_nl_kb_der_c16 in the reference layouts: natom(ntype),
+    rat(3, mxdatm, ntype), vkb(-2:nq, 0:3, -1:1, ntype) and nkb(0:3, -1:1, ntype) (spin-orbit
+    channel 0 filled), nanl, an xnlkb buffer, rkpt, adot, nqnl(ntype), delqnl(ntype)."""
+    ntype = len(species)
+    natom = np.array([sp.natom for sp in species], dtype=np.int32)
+    mxdatm = max(1, int(natom.max()) if ntype else 1)
+    rat = np.zeros((3, mxdatm, max(ntype, 1)), order="F")
+    for t, sp in enumerate(species):
+        if sp.natom:
+            rat[:, :sp.natom, t] = np.asarray(sp.rat, dtype=np.float64).T
+    vkb = np.asarray(vkb, dtype=np.float64)
+    vref = np.zeros((nq + 3, 4, 3, max(ntype, 1)), order="F")
+    nref = np.zeros((4, 3, max(ntype, 1)), dtype=np.int32, order="F")
+    for t in range(ntype):
+        for l in range(4):
+            vref[:, l, 1, t] = vkb[t, l, :nq + 3]
+            nref[l, 1, t] = int(nkb[t, l])
+    nanl = pseudo.nanl_of(species, np.asarray(nkb))
+    xnl = np.zeros(max(nanl, 1))
+    rk = np.ascontiguousarray(rkpt, dtype=np.float64)
+    ad = np.asfortranarray(adot, dtype=np.float64)
+    nqa = np.full(max(ntype, 1), nq, dtype=np.int32)
+    dqa = np.full(max(ntype, 1), delq, dtype=np.float64)
+    return ntype, natom, rat, mxdatm, vref, nref, nanl, xnl, rk, ad, nqa, dqa
+
+
 class Context:
     """One k-point's device state; H|psi> on device-resident complex128 torch tensors."""
 
@@ -165,26 +192,8 @@ class Context:
         reference layouts vkb(-2:nq, 0:3, -1:1, ntype) and nkb(0:3, -1:1, ntype) (spin-orbit
         channel 0). anlga_out: optional complex128 CUDA tensor (mtxd, nanl) column-major that
         receives a copy. Returns xnlkb (numpy)."""
-        ntype = len(species)
-        natom = np.array([sp.natom for sp in species], dtype=np.int32)
-        mxdatm = max(1, int(natom.max()) if ntype else 1)
-        rat = np.zeros((3, mxdatm, max(ntype, 1)), order="F")
-        for t, sp in enumerate(species):
-            if sp.natom:
-                rat[:, :sp.natom, t] = np.asarray(sp.rat, dtype=np.float64).T
-        vkb = np.asarray(vkb, dtype=np.float64)
-        vref = np.zeros((nq + 3, 4, 3, max(ntype, 1)), order="F")
-        nref = np.zeros((4, 3, max(ntype, 1)), dtype=np.int32, order="F")
-        for t in range(ntype):
-            for l in range(4):
-                vref[:, l, 1, t] = vkb[t, l, :nq + 3]
-                nref[l, 1, t] = int(nkb[t, l])
-        nanl = pseudo.nanl_of(species, np.asarray(nkb))
-        xnl = np.zeros(max(nanl, 1))
-        rk = np.ascontiguousarray(rkpt, dtype=np.float64)
-        ad = np.asfortranarray(adot, dtype=np.float64)
-        nqa = np.full(max(ntype, 1), nq, dtype=np.int32)
-        dqa = np.full(max(ntype, 1), delq, dtype=np.float64)
+        ntype, natom, rat, mxdatm, vref, nref, nanl, xnl, rk, ad, nqa, dqa = _kb_arrays(rkpt, species, vkb, nkb, adot,
+                                                                                    delq, nq)
         out_ptr, ld = None, 0
         if anlga_out is not None:
             if anlga_out.stride(0) != 1:
@@ -196,6 +205,31 @@ class Context:
                                                  dptr(xnl), out_ptr, ld))
         self.nanl = nanl
         return xnl[:nanl]
+
+    def proj_nl_kb_der(self, rkpt, species, vkb, nkb, adot, nder: int = 2, delq: float = 0.01, nq: int = 4000):
+        """Projectors of the current k-point and their derivatives with respect to the k-point's
+        lattice coordinates on the device (cpw_b200_proj_nl_kb_der_device, the device form of
+        Src/omp/proj_nl_kb_der_c16.f90). Returns (anlga (mtxd, nanl), danlgadrk (mtxd, nanl, 3) or
+        None, d2anlgadrk2 (mtxd, nanl, 3, 3) or None) as complex128 CUDA tensors in the reference
+        layouts (Fortran order), and xnlkb (numpy). The context's projectors are not changed."""
+        import torch
+        ntype, natom, rat, mxdatm, vref, nref, nanl, xnl, rk, ad, nqa, dqa = _kb_arrays(rkpt, species, vkb, nkb, adot,
+                                                                                    delq, nq)
+        m = self.mtxd
+        dev = torch.device("cuda", self.device)
+        # Fortran-order buffers: a flat tensor viewed with the reference's strides
+        a = torch.zeros(max(m * nanl, 1), dtype=torch.complex128, device=dev)
+        da = torch.zeros(max(m * nanl * 3, 1) if nder > 0 else 1, dtype=torch.complex128, device=dev)
+        d2a = torch.zeros(max(m * nanl * 9, 1) if nder > 1 else 1, dtype=torch.complex128, device=dev)
+        check(self._L.cpw_b200_proj_nl_kb_der_device(
+            self.handle, int(nder), dptr(rk), ntype, iptr(natom), dptr(rat), mxdatm, dptr(ad), iptr(nqa), dptr(dqa),
+            dptr(vref), nq, iptr(nref), nanl, dptr(xnl), C.c_void_p(a.data_ptr()), max(m, 1), max(nanl, 1),
+            C.c_void_p(da.data_ptr()) if nder > 0 else None, C.c_void_p(d2a.data_ptr()) if nder > 1 else None))
+        torch.cuda.synchronize(dev)
+        A = a[: m * nanl].as_strided((m, nanl), (1, m))
+        DA = da[: m * nanl * 3].as_strided((m, nanl, 3), (1, m, m * nanl)) if nder > 0 else None
+        D2A = d2a[: m * nanl * 9].as_strided((m, nanl, 3, 3), (1, m, m * nanl, 3 * m * nanl)) if nder > 1 else None
+        return A, DA, D2A, xnl[:nanl]
 
     def pot_local(self, veff, kgv, inds, phase=None, conj=None, kmscr=(0, 0, 0), idshift: int = 0,
                   install: bool = True, want_vscr: bool = True):

@@ -11,6 +11,7 @@ The ctypes calls release the GIL for their whole duration.
 """
 from __future__ import annotations
 
+import os
 import queue
 import threading
 import time
@@ -22,11 +23,17 @@ from .hk_psi import FP64, Context
 
 
 def eigensolve_kpoints(inputs: list[dict], nbands: int, workers: int = 8, precision: int = FP64, epspsi=1e-5,
-                       icmax=60, device: int = 0, seed: int = 0):
+                       icmax=60, device: int = 0, seed: int = 0, mxdbnd: int | None = None, trace: bool = False,
+                       keep: int = 0, slab_budget: int = 0, env: dict | None = None):
     """Run ditsp for every k-point dict of ``inputs`` (configs.kpoint_inputs(..., with_hamsm=True)).
 
     Returns (results, seconds): results[k] = dict(ei, neig, ihkpsum, converged) in input order,
     seconds the wall time of the whole set (inputs already on the host, contexts created inside).
+    mxdbnd: columns of psi/hpsi (default nbands; the reference's array dimension, which bounds
+    the iterative block). trace: also the per-iteration trace of each k-point (eigensolve's), with
+    times from the common start of the set. keep: the first ``keep`` columns of each k-point's
+    converged psi are returned (device tensors, ``psi``). slab_budget: FFT slab bytes per context.
+    env: environment variables set while the set runs (the eigensolver reads its switches then).
     """
     import torch
     dev = torch.device("cuda", device)
@@ -36,7 +43,13 @@ def eigensolve_kpoints(inputs: list[dict], nbands: int, workers: int = 8, precis
     results: list = [None] * len(inputs)
     errors: list = []
     nw = max(1, min(int(workers), len(inputs)))
+    mxdbnd = int(mxdbnd or nbands)
+    saved = {k: os.environ.get(k) for k in (env or {})}
+    os.environ.update(env or {})
     ctxs = [Context(device, precision=precision) for _ in range(nw)]
+    if slab_budget:
+        for c in ctxs:
+            c.set_slab_budget(slab_budget)
     # size every context's basis buffers for the largest k-point before the clock starts
     big = max(range(len(inputs)), key=lambda k: inputs[k]["mtxd"])
     for c in ctxs:
@@ -54,11 +67,17 @@ def eigensolve_kpoints(inputs: list[dict], nbands: int, workers: int = 8, precis
                 d = inputs[k]
                 ctx.setup(d)
                 with torch.cuda.stream(stream):
-                    psi = torch.zeros((nbands, d["mtxd"]), dtype=torch.complex128, device=dev).t()
+                    psi = torch.zeros((mxdbnd, d["mtxd"]), dtype=torch.complex128, device=dev).t()
                     hpsi = torch.zeros_like(psi)
+                    t_k = time.perf_counter() - t0
                     r = E.eigensolve(ctx, psi, hpsi, nbands, d["mtxds"], d["hamsm"], d["hdiag"], epspsi=epspsi,
-                                     icmax=icmax, stream=stream.cuda_stream)
+                                     icmax=icmax, stream=stream.cuda_stream, trace=trace)
                 stream.synchronize()
+                if trace:
+                    r["trace"][:, 0] += t_k          # times from the start of the set
+                if keep:
+                    r["psi"] = psi[:, :keep].clone()
+                del psi, hpsi
                 results[k] = r
         except Exception as exc:            # reported to the caller after the join
             errors.append(exc)
@@ -73,6 +92,11 @@ def eigensolve_kpoints(inputs: list[dict], nbands: int, workers: int = 8, precis
     seconds = time.perf_counter() - t0
     for c in ctxs:
         c.close()
+    for k, v in saved.items():
+        if v is None:
+            os.environ.pop(k, None)
+        else:
+            os.environ[k] = v
     if errors:
         raise errors[0]
     return results, seconds

@@ -125,6 +125,20 @@ int cpw_b200_proj_nl_kb_device(cpw_b200_ctx* ctx, const double* rkpt, int ntype,
                                const double* delqnl, const double* vkb, int mxdlqp, const int* nkb, int nanl,
                                double* xnlkb, void* anlga, long long ldanl);
 
+/* KB projectors and their derivatives with respect to the k-point's lattice
+ * coordinates, on the device: replaces Src/omp/proj_nl_kb_der_c16.f90:25-417
+ * (same inputs as cpw_b200_proj_nl_kb_device, nder = 0, 1 or 2). Outputs are
+ * device complex128 arrays in the reference layouts: anlga(ld, mxdanl),
+ * danlgadrk(ld, mxdanl, 3) for nder >= 1 and d2anlgadrk2(ld, mxdanl, 3, 3) for
+ * nder = 2 (ld >= mtxd, mxdanl >= nanl; the arrays a lower nder does not need
+ * may be NULL); xnlkb (host, may be NULL). The basis is the context's k-point;
+ * the context's own projectors are not changed. Synchronous. */
+int cpw_b200_proj_nl_kb_der_device(cpw_b200_ctx* ctx, int nder, const double* rkpt, int ntype, const int* natom,
+                                   const double* rat, int mxdatm, const double* adot, const int* nqnl,
+                                   const double* delqnl, const double* vkb, int mxdlqp, const int* nkb, int nanl,
+                                   double* xnlkb, void* anlga, long long ld, long long mxdanl, void* danlgadrk,
+                                   void* d2anlgadrk2);
+
 /* Screened local potential on the FFT mesh, computed on the device: replaces
  * Src/cpw_lib/pot_local.f90:1-190 (same arguments and array layouts, host
  * arrays: veff(mxdnst) complex(8) per star, kmscr(7) in/out (kmscr(4:7) set to

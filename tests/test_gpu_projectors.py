@@ -140,3 +140,32 @@ def test_no_projectors(cuda):
     want = O.hk_psi_c16(d["mtxd"], 3, psi, d["ekpg"], d["isort"], d["vscr"], d["kmscr"], d["kgv"],
                         np.zeros((d["mtxd"], 0), complex), np.zeros(0))
     assert relerr(y.cpu().numpy(), want) < TOL
+
+
+@pytest.mark.parametrize("ik,nder", [(2, 2), (0, 2), (3, 1), (1, 0)])
+def test_projector_k_derivatives_match_restatement(cuda, ik, nder):
+    # Src/omp/proj_nl_kb_der_c16.f90 on the device against oracle/projectors.py (itself pinned by
+    # finite differences on the CPU): s, p, d and f channels, three atom types, Gamma included
+    # (the |k+G| = 0 branch of the second derivative)
+    from oracle import projectors as OP
+    w = configs.WORKLOADS["si2"]()
+    species = [pseudo.Species(v0=sp.v0, sigma=sp.sigma, ekb=(2.0, -1.5, 0.7, -0.3), sigma_kb=0.9, rat=sp.rat)
+               for sp in w.species]
+    species.append(pseudo.Species(v0=1.0, sigma=0.7, ekb=(0.0, 1.1), sigma_kb=0.8, rat=np.array([[0.3, 0.1, 0.2]])))
+    d = configs.kpoint_inputs(w, ik)
+    vkb, nkb = pseudo.kb_tables(species, 0.01, 4000, lmax=3)
+    nt = len(species)
+    a, x, da, d2a = OP.proj_nl_kb_der_c16(d["rkpt"], d["isort"], d["kgv"], [sp.rat for sp in species], vkb, nkb,
+                                          np.full(nt, 4000), np.full(nt, 0.01), w.adot, nder)
+    ctx = H.Context(0)
+    ctx.set_kpoint(d["mtxd"], d["isort"], d["kgv"], d["ekpg"], d["kmscr"])
+    A, DA, D2A, xnl = ctx.proj_nl_kb_der(d["rkpt"], species, vkb, nkb, w.adot, nder=nder)
+    assert relerr(A.cpu().numpy(), a) < TOL
+    assert np.array_equal(xnl, x)
+    if nder > 0:
+        assert relerr(DA.cpu().numpy(), da) < TOL
+    else:
+        assert DA is None
+    if nder > 1:
+        assert relerr(D2A.cpu().numpy(), d2a) < TOL
+    ctx.close()
