@@ -125,7 +125,7 @@ def cpu_reference_rate(d, nbands: int, nthreads: int = 0, repeats: int = 1):
     return nbands / min(times), (nthreads or c_ref.max_threads())
 
 
-def time_to_eigvals(w, inputs, local, repeats=3, workers=4, icmax=400, nocc=None):
+def time_to_eigvals(w, inputs, local, repeats=3, workers=4, icmax=300, nocc=None, budget_s=480.0):
     """Eigensolver (ditsp_c16 restated) on the k-points of the Si216 workload, FP64 drop-in vs mixed.
 
     Each repeat solves every k-point of ``inputs`` (Gamma + 3 random k) from the start basis
@@ -135,8 +135,11 @@ def time_to_eigvals(w, inputs, local, repeats=3, workers=4, icmax=400, nocc=None
     time from the start of the set until every k-point's lowest nocc (occupied) Ritz values are
     within the tolerance of the reference values (the latest of the k-points' first such outer
     iteration). Reported as the median over repeats with the spread, at 1e-6 Ha for both forms
-    and 1e-8 Ha for FP64. Forces: adjoint (Hellmann-Feynman) forces at Gamma from each form's
-    converged occupied wavefunctions; their largest difference in Ha/bohr.
+    and 1e-8 Ha for FP64. The first repeat runs icmax outer iterations (its last values are the
+    reference); later repeats stop a few iterations after the first repeat reached the
+    tolerances, and start only while the eigensolver sets stay within budget_s seconds (the
+    number of repeats done is reported). Forces: adjoint (Hellmann-Feynman) forces at Gamma from
+    each form's converged occupied wavefunctions; their largest difference in Ha/bohr.
     """
     import torch
 
@@ -148,10 +151,14 @@ def time_to_eigvals(w, inputs, local, repeats=3, workers=4, icmax=400, nocc=None
     forms = (("fp64", H.FP64), ("mixed_tc", H.MIXED_TC))
     runs = {name: [] for name, _ in forms}
     keep = {}
+    icmax_rep = {name: icmax for name, _ in forms}
+    t_start = time.perf_counter()
+    refs = None
     for rep in range(repeats):
+        t_rep = time.perf_counter()
         for name, prec in forms:
             res, secs = kpoints.eigensolve_kpoints(inputs, NB, workers=workers, precision=prec, epspsi=1e-5,
-                                                   icmax=icmax, device=local, mxdbnd=3 * NB, trace=True,
+                                                   icmax=icmax_rep[name], device=local, mxdbnd=3 * NB, trace=True,
                                                    keep=nocc if rep == 0 else 0, slab_budget=2 << 30)
             if rep == 0:
                 keep[name] = res[0].pop("psi")
@@ -159,7 +166,20 @@ def time_to_eigvals(w, inputs, local, repeats=3, workers=4, icmax=400, nocc=None
                     r.pop("psi", None)
             runs[name].append((res, secs))
             torch.cuda.empty_cache()
-    refs = [r["trace"][-1, 4:4 + nocc] for r in runs["fp64"][0][0]]
+        if rep == 0:
+            refs = [r["trace"][-1, 4:4 + nocc] for r in runs["fp64"][0][0]]
+            # later repeats stop a few iterations after the first one met its tolerances
+            for name, _ in forms:
+                tol = 1e-8 if name == "fp64" else 1e-6
+                last = 0
+                for r, ref in zip(runs[name][0][0], refs):
+                    err = np.abs(r["trace"][:, 4:4 + nocc] - ref[None, :]).max(axis=1)
+                    ok = np.nonzero(err <= tol)[0]
+                    last = max(last, int(ok[0]) + 1 if len(ok) else r["trace"].shape[0])
+                icmax_rep[name] = min(icmax, last + 5)
+        dt = time.perf_counter() - t_rep
+        if time.perf_counter() - t_start + 0.8 * dt > budget_s:
+            break
 
     def set_time(res, tol):
         ts, its, hk = [], [], 0
@@ -174,8 +194,9 @@ def time_to_eigvals(w, inputs, local, repeats=3, workers=4, icmax=400, nocc=None
         return max(ts), its, hk
 
     out = {"kpoints": [[float(x) for x in w.kpoints[k]] for k in range(len(inputs))],
-           "mtxd": [int(d["mtxd"]) for d in inputs], "occupied": nocc, "repeats": repeats,
-           "kpoints_in_flight": workers}
+           "mtxd": [int(d["mtxd"]) for d in inputs], "occupied": nocc, "repeats": len(runs["fp64"]),
+           "repeats_asked": repeats, "kpoints_in_flight": workers, "icmax_first": icmax,
+           "icmax_later": icmax_rep}
     for name, _ in forms:
         tols = (1e-6, 1e-8) if name == "fp64" else (1e-6,)
         entry = {}
@@ -611,7 +632,8 @@ def run_ours(args, world, rank, local, dist):
     line["kbatch"] = kbatch_throughput(local, max(3, args.steps // 2), 2)
     if args.eig:
         line["time_to_eigvals"] = time_to_eigvals(w, inputs, local, repeats=args.eig_repeats,
-                                                  workers=min(args.eig_workers, len(inputs)))
+                                                  workers=min(args.eig_workers, len(inputs)),
+                                                  budget_s=args.eig_budget)
     if rank == 0 and world == 1:
         rate, cores = cpu_reference_rate(d, REF_SAMPLE, repeats=2)
         line["cpu_baseline"] = {"value": rate, "unit": "bands/s", "cores": cores, "kind": "port",
@@ -698,6 +720,7 @@ def main():
     ap.add_argument("--eig-repeats", type=int, default=3, help="repeats of the time-to-eigvals sets (median)")
     ap.add_argument("--eig-kpoints", type=int, default=4, help="k-points of the Si216 workload solved (Gamma first)")
     ap.add_argument("--eig-workers", type=int, default=4, help="k-points in flight during the eigensolver sets")
+    ap.add_argument("--eig-budget", type=float, default=480.0, help="seconds the eigensolver repeats may take")
     args = ap.parse_args()
     world, rank, local, dist = dist_setup(args)
     try:
