@@ -31,6 +31,7 @@ SIGNATURES = {
     "cpw_b200_set_slab_budget": (I, [P, LL]),
     "cpw_b200_set_wait_limits": (I, [P, LL, LL]),
     "cpw_b200_wait_selftest": (I, [P, LL, P]),
+    "cpw_b200_zgemm_i8": (I, [P, I, I, I, I, P, LL, P, LL, C.c_double, I, P, LL, I, P]),
     "cpw_b200_timing_begin": (I, [P]),
     "cpw_b200_timing_end": (I, [P, DP, C.POINTER(C.c_longlong), I]),
     "cpw_b200_set_kpoint": (I, [P, I, IP, IP, I, DP, IP]),

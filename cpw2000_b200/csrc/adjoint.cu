@@ -291,7 +291,7 @@ int density_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, co
   if ((e = cudaMemcpyAsync(docc.p, occ, sizeof(double) * nb, cudaMemcpyHostToDevice, st)) != cudaSuccess)
     return cuda_fail(e, "density occ");
   const size_t sm = (sizeof(C2<double>) + sizeof(double)) * (size_t)p.n3 * kDensCB + sizeof(C2<double>) * p.n3;
-  if ((e = cudaFuncSetAttribute(k_dens_z, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != cudaSuccess)
+  if ((e = smem_limit((const void*)k_dens_z, (size_t)sm)) != cudaSuccess)
     return cuda_fail(e, "density attribute");
   for (int b0 = 0; b0 < nb; b0 += chunk) {
     const int nbc = std::min(chunk, nb - b0);
@@ -340,7 +340,7 @@ int structure_grad_device(cpw_b200_ctx* c, const void* g, int natom, const int* 
   }
   const size_t sm = sizeof(Z) * ((size_t)p.n1 + p.n2 + p.n3);
   if (natom > 0) {
-    cudaFuncSetAttribute(k_structure_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    smem_limit((const void*)k_structure_grad, (size_t)sm);
     k_structure_grad<<<natom, 256, sm, st>>>(p.n1, p.n2, p.n3, (const Z*)fg.p, (const double*)vgt,
                                              (const int*)dtype.p, (const double*)dtau.p, (double*)dout.p);
     e = cudaMemcpyAsync(dedtau, dout.p, sizeof(double) * 3 * natom, cudaMemcpyDeviceToHost, st);

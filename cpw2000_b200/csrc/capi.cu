@@ -454,6 +454,19 @@ int cpw_b200_wait_selftest(cpw_b200_ctx* c, long long limit_ns, void* stream) {
   return tc_wait_selftest(c, (unsigned long long)limit_ns, stream ? (cudaStream_t)stream : c->stream);
 }
 
+int cpw_b200_zgemm_i8(cpw_b200_ctx* c, int transa, int m, int n, int k, const void* a, long long lda, const void* b,
+                      long long ldb, double alpha, int accumulate, void* cm, long long ldc, int slices, void* stream) {
+  if (int s = check_ctx(c)) return s;
+  if (transa != 'N' && transa != 'C') return fail(kBadArg, "zgemm_i8: transa must be 'N' or 'C'");
+  if (m < 0 || n < 0 || k < 0) return fail(kBadArg, "zgemm_i8: negative dimension");
+  const bool conj = transa == 'C';
+  if ((conj ? lda < std::max(k, 1) : lda < std::max(m, 1)) || ldb < std::max(k, 1) || ldc < std::max(m, 1))
+    return fail(kBadArg, "zgemm_i8: leading dimension too small");
+  cudaSetDevice(c->device);
+  return oz_zgemm(c->ozs, conj, m, n, k, a, lda, b, ldb, alpha, accumulate != 0, cm, ldc, slices, c->tcs.wait_ns,
+                  stream ? (cudaStream_t)stream : c->stream);
+}
+
 int cpw_b200_timing_begin(cpw_b200_ctx* c) {
   if (int s = check_ctx(c)) return s;
   c->timer.on = true;

@@ -74,6 +74,17 @@ struct TcScratch {
   unsigned long long wait_ns = 2000000000ull;   // hand-off wait limit of the tensor-core GEMMs
 };
 int tc_wait_selftest(cpw_b200_ctx* c, unsigned long long limit_ns, cudaStream_t st);
+// work space of the int8 tensor-core (Ozaki) complex GEMM and its sticky error flag
+struct OzScratch {
+  DevBuf a, b, ea, eb, sa, sb, part, err;
+  bool err_init = false;
+};
+// C = alpha op(A) B (+ C) with op(A) = A or A^H, complex128 column-major, FP64-accurate on the
+// int8 tensor cores with `slices` 7-bit slices per operand (oz.cu)
+int oz_zgemm(OzScratch& w, bool conjA, int M, int N, int K, const void* A, long long lda, const void* B, long long ldb,
+             double alpha, bool accumulate, void* C, long long ldc, int slices, unsigned long long wait_ns,
+             cudaStream_t st);
+int oz_read_error(OzScratch& w);
 int tc_error_flag(TcScratch& t);
 int tc_read_error(TcScratch& t);
 int tc_prepare_projectors(cpw_b200_ctx* c);
@@ -133,6 +144,7 @@ struct cpw_b200_ctx {
   // mixed precision: split-TF32 operands of the tensor-core projector GEMMs
   cpwb::DevBuf tc_a1, tc_a2, tc_ga, tc_gb;
   cpwb::TcScratch tcs;
+  cpwb::OzScratch ozs;          // int8 tensor-core GEMMs of the eigensolver's basis products
   long long tc_k1p = 0, tc_k2p = 0;     // K blocks (32 reals) of the projection and expansion operands
   bool tc_ready = false;
 

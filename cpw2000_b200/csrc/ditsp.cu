@@ -282,6 +282,16 @@ __global__ void k_diag_re(const Z* __restrict__ G, int k, double* __restrict__ o
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) out[i] = G[(size_t)i * k + i].x;
 }
 
+// out = A^H for a k x k column-major matrix
+__global__ void k_conj_transpose(const Z* __restrict__ A, int k, Z* __restrict__ out) {
+  const long long n = (long long)k * k;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(t % k), c = (int)(t / k);
+    const Z v = A[(size_t)r * k + c];
+    out[t] = make_cuDoubleComplex(v.x, -v.y);
+  }
+}
+
 // zero the strictly upper triangle of a k x k column-major matrix
 __global__ void k_zero_upper(Z* G, int k) {
   const long long n = (long long)k * k;
@@ -360,10 +370,26 @@ struct Solver {
     return ctx_hkpsi_device(c, n, x, ldx, hx, ldhx, st, true, true);
   }
 
+  // Basis-wide products of the mixed forms on the int8 tensor cores (FP64-accurate Ozaki GEMM,
+  // oz.cu) instead of cuBLAS FP64; products below kI8MinFlops stay in cuBLAS (the splitting
+  // launches cost more than they save there)
+  bool basis_i8 = false;
+  int oz_slices = 7;
+  long long n_i8 = 0, n_cublas = 0;
+  static constexpr double kI8MinFlops = 2e9;
+
   // C(m x n) = alpha * op(A) * op(B) + beta * C
   int gemm(cublasOperation_t ta, cublasOperation_t tb, int mm, int nn, int kk, Z alpha, const Z* A, long long lda,
            const Z* Bm, long long ldb, Z beta, Z* Cm, long long ldc, const char* w) {
     if (mm <= 0 || nn <= 0) return kOk;
+    if (basis_i8 && kk > 0 && tb == CUBLAS_OP_N && (ta == CUBLAS_OP_N || ta == CUBLAS_OP_C) && alpha.y == 0 &&
+        (alpha.x == 1.0 || alpha.x == -1.0) && beta.y == 0 && (beta.x == 0.0 || beta.x == 1.0) &&
+        8.0 * mm * nn * kk >= kI8MinFlops) {
+      ++n_i8;
+      return oz_zgemm(c->ozs, ta == CUBLAS_OP_C, mm, nn, kk, A, lda, Bm, ldb, alpha.x, beta.x != 0.0, Cm, ldc,
+                      oz_slices, c->tcs.wait_ns, st);
+    }
+    ++n_cublas;
     if (kk <= 0) {
       // C = beta C
       if (beta.x == 0 && beta.y == 0) {
@@ -468,11 +494,12 @@ struct Solver {
   DevBuf ham_prev;
   void touch(int c0) { ham_clean = std::max(0, std::min(ham_clean, c0)); }
   bool chol = false;
+  bool ham_full_gemm = false;  // Ritz subspace Hamiltonian block as a full product instead of zherkx
   bool partial_eig = false;    // Ritz step: only the eigenpairs its decisions and rotations read
   long long n_eig_full_again = 0;
   bool tc_rot = false;   // Ritz rotations on the tensor cores (mixed form with tensor-core projectors)
   long long n_chol = 0, n_chol_fallback = 0, n_fb_info = 0, n_fb_drop = 0, n_fb_cond = 0;
-  DevBuf chol_g, chol_work, chol_info, chol_idx, chol_diag, chol_tmp, chol_tri;
+  DevBuf chol_g, chol_work, chol_info, chol_idx, chol_diag, chol_tmp, chol_tri, chol_lh;
   bool chol_gram_gemm = true, chol_apply_gemm = true;
   // L (lower, k x k in G) -> L^-1 in place, strictly upper part zeroed
   int chol_inverse(Z* G, int k) {
@@ -496,7 +523,17 @@ struct Solver {
   int apply_right_lh(Z* x, int k, const Z* Li) {
     if (int s = chol_tmp.ensure(sizeof(Z) * (size_t)m * k)) return s;
     Z* t = (Z*)chol_tmp.p;
-    if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_C, m, k, k, one, x, m, Li, k, zero, t, m, "cholqr apply")) return s;
+    if (basis_i8) {
+      // the int8 GEMM takes B as stored: form Li^H
+      if (int s = chol_lh.ensure(sizeof(Z) * (size_t)k * k)) return s;
+      k_conj_transpose<<<std::max(1, std::min(1184, (int)(((long long)k * k + 255) / 256))), 256, 0, st>>>(
+          Li, k, (Z*)chol_lh.p);
+      if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_N, m, k, k, one, x, m, (const Z*)chol_lh.p, k, zero, t, m,
+                       "cholqr apply"))
+        return s;
+    } else if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_C, m, k, k, one, x, m, Li, k, zero, t, m, "cholqr apply")) {
+      return s;
+    }
     return ck(cudaMemcpyAsync(x, t, sizeof(Z) * (size_t)m * k, cudaMemcpyDeviceToDevice, st), "cholqr apply");
   }
   // the real diagonal of G (k x k) into host h (k doubles)
@@ -839,13 +876,13 @@ struct Solver {
 // would serialise contexts that solve different k-points at the same time.
 struct SolverPool {
   Solver& S;
-  static constexpr int kN = 23;
+  static constexpr int kN = 24;
   DevBuf* m[kN];
   explicit SolverPool(Solver& s) : S(s) {
     DevBuf* l[kN] = {&S.bas,  &S.hbas,      &S.smallA,    &S.smallV,   &S.dvec,     &S.dvec2,    &S.dz,
                      &S.work, &S.info,      &S.eg_d,      &S.hdiag_d,  &S.ham_prev, &S.chol_g,   &S.chol_work,
                      &S.chol_info, &S.chol_idx, &S.mgs_part, &S.mgs_bar, &S.mgs_irow, &S.mgs_xscl, &S.chol_diag,
-                     &S.chol_tmp, &S.chol_tri};
+                     &S.chol_tmp, &S.chol_tri, &S.chol_lh};
     for (int i = 0; i < kN; ++i) {
       m[i] = l[i];
       swap(*m[i], S.c->ditsp_pool[i]);
@@ -926,6 +963,19 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
   // partial subspace eigensolve (zheevdx, lowest pairs only): measured no faster than zheevd on the
   // Si216 Ritz matrices (~1100), so off unless CPW_B200_EIG_PARTIAL=1
   S.partial_eig = getenv("CPW_B200_EIG_PARTIAL") && !strcmp(getenv("CPW_B200_EIG_PARTIAL"), "1");
+  // basis-wide products: FP64 cuBLAS in the drop-in, the FP64-accurate int8 tensor-core GEMM in the
+  // mixed forms; CPW_B200_BASIS_GEMM=fp64|i8 overrides, CPW_B200_OZ_SLICES sets its slices (1..8)
+  S.basis_i8 = c->precision != 0;
+  if (const char* v = getenv("CPW_B200_BASIS_GEMM")) {
+    if (!strcmp(v, "fp64")) S.basis_i8 = false;
+    if (!strcmp(v, "i8")) S.basis_i8 = true;
+  }
+  if (const char* v = getenv("CPW_B200_OZ_SLICES")) S.oz_slices = std::max(1, std::min(8, atoi(v)));
+  S.ham_full_gemm = S.basis_i8;
+  if (const char* v = getenv("CPW_B200_HAM_BLOCK")) {
+    if (!strcmp(v, "herkx")) S.ham_full_gemm = false;
+    if (!strcmp(v, "gemm")) S.ham_full_gemm = true;
+  }
   S.chol_gram_gemm = !(getenv("CPW_B200_CHOL_GRAM") && !strcmp(getenv("CPW_B200_CHOL_GRAM"), "herk"));
   S.chol_apply_gemm = !(getenv("CPW_B200_CHOL_APPLY") && !strcmp(getenv("CPW_B200_CHOL_APPLY"), "trsm"));
   if (const char* o = getenv("CPW_B200_ORTHO")) {
@@ -1330,10 +1380,16 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
                         S.zero, H + (size_t)cz * nsize + c, nsize, "ritz hamsm rows")))
             return s;
         const int d0 = std::max(c, cz);
-        if (d0 < nsize && cublasZherkx(S.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, nsize - d0, mtxd, &S.one,
-                                       S.HB(d0), mtxd, S.B(d0), mtxd, &b0, H + (size_t)d0 * nsize + d0,
-                                       nsize) != CUBLAS_STATUS_SUCCESS)
+        if (d0 < nsize && S.ham_full_gemm) {
+          // the whole square (twice the products of the triangle, at the full GEMM rate)
+          if ((s = S.gemm(CUBLAS_OP_C, CUBLAS_OP_N, nsize - d0, nsize - d0, mtxd, S.one, S.HB(d0), mtxd, S.B(d0),
+                          mtxd, S.zero, H + (size_t)d0 * nsize + d0, nsize, "ritz hamsm block")))
+            return s;
+        } else if (d0 < nsize && cublasZherkx(S.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, nsize - d0, mtxd, &S.one,
+                                              S.HB(d0), mtxd, S.B(d0), mtxd, &b0, H + (size_t)d0 * nsize + d0,
+                                              nsize) != CUBLAS_STATUS_SUCCESS) {
           return fail(kCublas, "ritz hamsm");
+        }
       }
       // keep it for the next Ritz step (zheevd overwrites smallV)
       if ((s = S.ham_prev.ensure(sizeof(Z) * (size_t)nsize * nsize)) ||
@@ -1426,7 +1482,7 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
     // to the first zrows rows only
     const int cz = std::min(S.zcols, nsize);
     const Z* V = (const Z*)S.smallV.p;
-    if (S.tc_rot) {
+    if (S.tc_rot && !S.basis_i8) {
       if ((s = tc_zgemm_nn(c, mtxd, niter, nsize - cz, S.B(cz), mtxd, V + cz, nsize, PP, mtxd, st)) ||
           (cz > 0 && (s = tc_zgemm_nn(c, S.zrows, niter, cz, S.bas.p, mtxd, V, nsize, PP, mtxd, st, true))) ||
           (s = tc_zgemm_nn(c, mtxd, niter, nsize, S.hbas.p, mtxd, S.smallV.p, nsize, HPP, mtxd, st)))
@@ -1501,11 +1557,13 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
            "Hamiltonian %.4f s (%lld reused leading blocks, %lld full), Ritz rotations + residual check %.4f s\n",
            S.tphase[5], S.tphase[6], S.tphase[7], S.tphase[8], S.ham_reused, S.ham_full, S.tphase[9]);
     printf("  ditsp_c16: Cholesky QR parts: Gram %.4f s, factorisation %.4f s, triangular solves %.4f s; "
-           "partial subspace eigensolves redone in full: %lld\n",
-           S.tphase[10], S.tphase[11], S.tphase[12], S.n_eig_full_again);
+           "partial subspace eigensolves redone in full: %lld; basis products: %lld int8 tensor-core (%d slices), "
+           "%lld cuBLAS\n",
+           S.tphase[10], S.tphase[11], S.tphase[12], S.n_eig_full_again, S.n_i8, S.oz_slices, S.n_cublas);
     fflush(stdout);
   }
   if ((s = S.ck(cudaStreamSynchronize(st), "ditsp"))) return s;
+  if (S.basis_i8 && (s = oz_read_error(c->ozs))) return s;
   return lconv ? kOk : kNotConverged;
 }
 

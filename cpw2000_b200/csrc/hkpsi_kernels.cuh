@@ -553,8 +553,8 @@ cudaError_t launch_impl(const LocalPlan& p, int nbc, int band0, const C2<double>
   auto* ka = k_inv_xy<T, RX1, RX2, RY1, RY2, TC, NTP>;
   auto* kc = k_fwd_xy<T, RX1, RX2, RY1, RY2, TC, NTC>;
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pl)) != cudaSuccess) return e;
-  if ((e = cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pl)) != cudaSuccess) return e;
+  if ((e = smem_limit((const void*)ka, (size_t)sm_pl)) != cudaSuccess) return e;
+  if ((e = smem_limit((const void*)kc, (size_t)sm_pl)) != cudaSuccess) return e;
   int nsm = 148, dev = 0, smax = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -569,7 +569,7 @@ cudaError_t launch_impl(const LocalPlan& p, int nbc, int band0, const C2<double>
     // the staged form does not fit: one CTA per (band, column tile)
     const size_t sm_co = smem_columns<T>(p);
     auto* kb = k_z_vloc<T, RZ1, RZ2, CB>;
-    if ((e = cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_co)) != cudaSuccess) return e;
+    if ((e = smem_limit((const void*)kb, (size_t)sm_co)) != cudaSuccess) return e;
     kb<<<dim3((unsigned)tiles, nbc), kThreadsCols, sm_co, st>>>(p, vr, twz, W);
   } else {
     // column tiles x band groups: enough CTAs for two per SM on small boxes
@@ -578,7 +578,7 @@ cudaError_t launch_impl(const LocalPlan& p, int nbc, int band0, const C2<double>
     const int per = (int)((nbc + groups - 1) / groups);
     groups = (nbc + per - 1) / per;
     auto* kbp = k_z_vloc_pipe<T, RZ1, RZ2, CB, NTZ>;
-    if ((e = cudaFuncSetAttribute(kbp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pipe)) != cudaSuccess)
+    if ((e = smem_limit((const void*)kbp, (size_t)sm_pipe)) != cudaSuccess)
       return e;
     kbp<<<dim3((unsigned)tiles, (unsigned)groups), NTZ, sm_pipe, st>>>(p, nbc, per, vr, twz, W);
   }
@@ -596,7 +596,7 @@ cudaError_t launch_inv_impl(const LocalPlan& p, int nbc, int band0, const C2<dou
   constexpr int NTP = TC && RY1 ? pass_threads(TC * RY2, TC * RY1) : kThreadsPlanes;
   const size_t sm_pl = smem_planes<T>(p);
   auto* ka = k_inv_xy<T, RX1, RX2, RY1, RY2, TC, NTP>;
-  cudaError_t e = cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pl);
+  cudaError_t e = smem_limit((const void*)ka, (size_t)sm_pl);
   if (e != cudaSuccess) return e;
   ka<<<dim3(p.nz, nbc), NTP, sm_pl, st>>>(p, band0, psi, ldpsi, plane_start, pw_idx, pw_pos, twx, twy, W);
   return cudaGetLastError();

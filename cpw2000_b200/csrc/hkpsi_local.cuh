@@ -20,9 +20,30 @@
 // table in shared memory.
 #pragma once
 #include <stdlib.h>
+
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "cplx.cuh"
 
 namespace cpwb {
+
+// Raise, never lower, the dynamic shared memory a kernel may take. Function attributes are
+// process-wide: host threads that launch one kernel with different sizes (contexts of different
+// k-points in flight) must not lower each other's limit between the setting and the launch.
+inline cudaError_t smem_limit(const void* f, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> cur;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& v = cur[{dev, f}];
+  if (bytes <= v) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) v = bytes;
+  return e;
+}
 
 struct FftDim {
   int n, r1, r2;

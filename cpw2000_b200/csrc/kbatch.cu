@@ -462,7 +462,7 @@ int cpw_b200_kbatch_hk_psi_device(cpw_b200_kbatch* b, const int* nb, void* const
       if (b->nl_batched) {
         b->nl_ptot = poff;
         b->nl_mmax = mmax;
-        cudaError_t ea = cudaFuncSetAttribute(k_batch_expand, cudaFuncAttributeMaxDynamicSharedMemorySize, kNlSmem);
+        cudaError_t ea = cpwb::smem_limit((const void*)k_batch_expand, (size_t)kNlSmem);
         if (ea != cudaSuccess) return cuda_fail(ea, "kbatch attribute");
         if ((s = cpwb::upload(b->nl_d, nd.data(), nd.size() * sizeof(NlDesc))) ||
             (s = b->nl_part.ensure((size_t)kNlSlices * poff * sizeof(C2<double>))) ||

@@ -759,10 +759,8 @@ int tc_nl_apply_ops(TcScratch& t, int m, int na, long long nkb1, long long nkb2,
   g2.wait_ns = t.wait_ns;
 
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(tc::k_gemm_tf32x3<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                tc::kSmemBytes)) != cudaSuccess ||
-      (e = cudaFuncSetAttribute(tc::k_gemm_tf32x3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                tc::kSmemBytes)) != cudaSuccess)
+  if ((e = smem_limit((const void*)tc::k_gemm_tf32x3<0>, (size_t)tc::kSmemBytes)) != cudaSuccess ||
+      (e = smem_limit((const void*)tc::k_gemm_tf32x3<1>, (size_t)tc::kSmemBytes)) != cudaSuccess)
     return cuda_fail(e, "tensor-core GEMM attribute");
   const int items1 = mt1 * nt1 * nsplit, items2 = mt2 * nt2;
   if (t0) cudaEventRecord(t0, st);
@@ -833,15 +831,17 @@ int tc_zgemm_nn(cpw_b200_ctx* c, int m, int n, int kk, const void* a, long long 
   g.ldh = ldc;
   g.err = (int*)c->tcs.err.p;
   g.wait_ns = c->tcs.wait_ns;
-  if ((e = cudaFuncSetAttribute(tc::k_gemm_tf32x3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                tc::kSmemBytes)) != cudaSuccess)
+  if ((e = smem_limit((const void*)tc::k_gemm_tf32x3<1>, (size_t)tc::kSmemBytes)) != cudaSuccess)
     return cuda_fail(e, "tensor-core GEMM attribute");
   tc::k_gemm_tf32x3<1><<<std::min(mt * nt, nsm), tc::kThreads, tc::kSmemBytes, st>>>(g);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "tensor-core zgemm");
   return kOk;
 }
 
-int tc_check_error(cpw_b200_ctx* c) { return tc_read_error(c->tcs); }
+int tc_check_error(cpw_b200_ctx* c) {
+  if (int s = tc_read_error(c->tcs)) return s;
+  return oz_read_error(c->ozs);
+}
 
 namespace tc {
 // Failure-detection self-test: one thread waits, through the same bounded wait as the GEMM

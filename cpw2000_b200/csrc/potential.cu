@@ -195,7 +195,7 @@ int ctx_pot_local(cpw_b200_ctx* c, int n1, int n2, int n3, int id, int ng, const
   for (int a = 0; a < 3; ++a) {
     const long long nlines = (long long)(ntot / ns[a]);
     const size_t sm = sizeof(C2<double>) * ((size_t)ns[a] * kLines + ns[a]);
-    if ((e = cudaFuncSetAttribute(k_lines_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != cudaSuccess)
+    if ((e = smem_limit((const void*)k_lines_backward, (size_t)sm)) != cudaSuccess)
       return cuda_fail(e, "pot_local attribute");
     k_lines_backward<<<(unsigned)((nlines + kLines - 1) / kLines), kThreads, sm, st>>>(
         (C2<double>*)box.p, dims[a], es[a], nfast[a], sfast[a], sslow[a], nlines, (const C2<double>*)tw[a].p);

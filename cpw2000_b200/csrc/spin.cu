@@ -201,10 +201,10 @@ int spin_local(cpw_b200_ctx* c, int nb, const C2<double>* psi, long long ldpsi, 
   W = (C2<T>*)c->slab.p;
   const size_t sm_pl = smem_planes<T>(p);
   auto* kc = kern::k_fwd_xy<T, 0, 0, 0, 0, 0>;
-  if ((e = cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pl)) != cudaSuccess)
+  if ((e = smem_limit((const void*)kc, (size_t)sm_pl)) != cudaSuccess)
     return cuda_fail(e, "hk_psi_spin attribute");
   const size_t sm_z = sizeof(C2<T>) * (2 * (size_t)p.n3 * kSpCols + p.n3);
-  if ((e = cudaFuncSetAttribute(k_z_spinor<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_z)) != cudaSuccess)
+  if ((e = smem_limit((const void*)k_z_spinor<T>, (size_t)sm_z)) != cudaSuccess)
     return cuda_fail(e, "hk_psi_spin attribute");
   const unsigned tiles = (unsigned)((p.plane + kSpCols - 1) / kSpCols);
   for (int b0 = 0; b0 < nb; b0 += chunk) {

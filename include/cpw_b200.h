@@ -89,6 +89,18 @@ int cpw_b200_set_slab_budget(cpw_b200_ctx* ctx, long long bytes);
 int cpw_b200_set_wait_limits(cpw_b200_ctx* ctx, long long mbarrier_ns, long long grid_polls);
 int cpw_b200_wait_selftest(cpw_b200_ctx* ctx, long long limit_ns, void* stream);
 
+/* FP64-accurate complex GEMM on the int8 tensor cores (no counterpart in the
+ * reference, whose ZGEMMs are BLAS calls): C = alpha op(A) B (+ C when
+ * accumulate != 0), op(A) = A (transa 'N', A m x k) or A^H (transa 'C', A k x
+ * m), B k x n; device complex128 column-major arrays, alpha real. Each operand
+ * row is split into `slices` (1..8) 7-bit integer slices under a power-of-two
+ * row scale (the Ozaki scheme); with 7 slices an entry's error is below ~2^-48
+ * k max|a| max|b|. Asynchronous on `stream` (NULL = the context stream); a
+ * bounded wait that gave up is reported by cpw_b200_synchronize. */
+int cpw_b200_zgemm_i8(cpw_b200_ctx* ctx, int transa, int m, int n, int k, const void* a, long long lda,
+                      const void* b, long long ldb, double alpha, int accumulate, void* c, long long ldc, int slices,
+                      void* stream);
+
 /* Stage timers (CUDA events around each kernel of a stage, on the stream the
  * kernel runs on). timing_end synchronises and writes per-stage totals in ms
  * and launch counts for stages 0..nstage-1: 0 scatter+inverse xy, 1 inverse z +

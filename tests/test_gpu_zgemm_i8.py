@@ -1,0 +1,92 @@
+"""FP64-accurate complex GEMM on the int8 tensor cores (cpw_b200_zgemm_i8, csrc/oz.cu) against
+an FP64 reference product (numpy complex128 on the CPU).
+
+Shapes of the eigensolver's basis products: tall-skinny Gram products A^H B with a long K
+(split over work items), rotations A B with a tall A, accumulation with alpha = -1 (the
+Gram-Schmidt update), ragged sizes (M, N, K not multiples of the tiles), and operands whose
+magnitudes decay by orders of magnitude along K (plane-wave coefficients of smooth bands).
+Tolerance: 1e-13 of max|C| with 7 slices (2^-48 relative to the row maxima); fewer slices
+lose 7 bits each, which the slice sweep checks.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from cpw2000_b200 import _lib
+from cpw2000_b200 import hk_psi as H
+
+pytestmark = pytest.mark.gpu
+
+
+def _rand(rng, shape, decay=0.0):
+    x = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    if decay:
+        x *= np.exp(-decay * np.linspace(0, 1, shape[0]))[:, None]
+    return np.asfortranarray(x)
+
+
+def _run(torch, dev, ctx, transa, a, b, m, n, k, alpha=1.0, c0=None, slices=7):
+    L = _lib.lib()
+    A = torch.from_numpy(np.ascontiguousarray(a.T)).to(dev).t()
+    B = torch.from_numpy(np.ascontiguousarray(b.T)).to(dev).t()
+    Cm = torch.zeros((n, m), dtype=torch.complex128, device=dev).t() if c0 is None else \
+        torch.from_numpy(np.ascontiguousarray(c0.T)).to(dev).t()
+    st = L.cpw_b200_zgemm_i8(ctx.handle, ord(transa), m, n, k, C.c_void_p(A.data_ptr()), int(A.stride(1)),
+                             C.c_void_p(B.data_ptr()), int(B.stride(1)), float(alpha), 0 if c0 is None else 1,
+                             C.c_void_p(Cm.data_ptr()), int(Cm.stride(1)), slices, None)
+    _lib.check(st)
+    ctx.synchronize()
+    return Cm.cpu().numpy()
+
+
+@pytest.mark.parametrize("transa,m,n,k,decay", [("C", 130, 70, 20000, 0.0), ("C", 257, 33, 178001, 8.0),
+                                                 ("N", 300, 45, 1000, 0.0), ("N", 1000, 17, 333, 5.0),
+                                                 ("C", 1, 1, 5, 0.0), ("N", 129, 65, 64, 0.0)])
+def test_zgemm_i8_matches_fp64(cuda, transa, m, n, k, decay):
+    import torch
+    rng = np.random.default_rng(m * 7 + n * 3 + k)
+    ctx = H.Context(0)
+    a = _rand(rng, (k, m) if transa == "C" else (m, k), decay if transa == "C" else 0.0)
+    b = _rand(rng, (k, n), decay)
+    got = _run(torch, cuda, ctx, transa, a, b, m, n, k)
+    ref = (a.conj().T if transa == "C" else a) @ b
+    err = np.abs(got - ref).max() / np.abs(ref).max()
+    assert err < 1e-13, f"relative error {err:.3e}"
+    ctx.close()
+
+
+def test_zgemm_i8_accumulate_and_alpha(cuda):
+    import torch
+    rng = np.random.default_rng(5)
+    ctx = H.Context(0)
+    m, n, k = 700, 40, 90
+    a, b, c0 = _rand(rng, (m, k)), _rand(rng, (k, n)), _rand(rng, (m, n))
+    got = _run(torch, cuda, ctx, "N", a, b, m, n, k, alpha=-1.0, c0=c0)
+    ref = c0 - a @ b
+    assert np.abs(got - ref).max() / np.abs(ref).max() < 1e-13
+    # long K (split into FP64 partials) with accumulation
+    m, n, k = 96, 50, 150000
+    a, b, c0 = _rand(rng, (k, m)), _rand(rng, (k, n)), _rand(rng, (m, n))
+    got = _run(torch, cuda, ctx, "C", a, b, m, n, k, alpha=-1.0, c0=c0)
+    ref = c0 - a.conj().T @ b
+    assert np.abs(got - ref).max() / np.abs(ref).max() < 1e-13
+    ctx.close()
+
+
+def test_zgemm_i8_error_shrinks_with_slices(cuda):
+    import torch
+    rng = np.random.default_rng(9)
+    ctx = H.Context(0)
+    m, n, k = 64, 24, 4000
+    a, b = _rand(rng, (k, m)), _rand(rng, (k, n))
+    ref = a.conj().T @ b
+    errs = []
+    for s in (2, 3, 4, 5, 6, 7):
+        got = _run(torch, cuda, ctx, "C", a, b, m, n, k, slices=s)
+        errs.append(np.abs(got - ref).max() / np.abs(ref).max())
+    # each slice adds 7 bits: the error falls by orders of magnitude until FP64 rounding
+    for s, e in zip((2, 3, 4, 5, 6), errs):
+        assert e < 2.0 ** (-(6 + 7 * (s - 1)) + 8), (s, e)
+    assert errs[-1] < 1e-13
+    ctx.close()
