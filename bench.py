@@ -678,6 +678,65 @@ def si64_throughput(local, steps, warmup):
     return out
 
 
+def run_gemm(args, local):
+    """The eigensolver's basis-product shapes on the int8 tensor cores (cpw_b200_zgemm_i8, 7 slices)
+    against cuBLAS ZGEMM (torch complex128 matmul): median ms of --steps calls after --warmup."""
+    import ctypes as C
+
+    import torch
+
+    from cpw2000_b200 import _lib
+    from cpw2000_b200 import hk_psi as H
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ctx = H.Context(local)
+    L = _lib.lib()
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    st = stream.cuda_stream
+    shapes = [("C", 1000, 180, 88951), ("N", 88951, 180, 1000), ("C", 180, 180, 88951), ("N", 88951, 490, 1160),
+              ("C", 864, 480, 88951), ("N", 88951, 480, 864)]
+    out = {"mode": "gemm", "slices": args.slices, "shapes": []}
+    for ta, m, n, k in shapes[: args.nshapes]:
+        a = torch.randn((k, m) if ta == "C" else (m, k), dtype=torch.complex128, device=dev)
+        a = a.t().contiguous().t()                   # column-major
+        b = torch.randn((k, n), dtype=torch.complex128, device=dev).t().contiguous().t()
+        c = torch.zeros((n, m), dtype=torch.complex128, device=dev).t()
+        lda = a.shape[0]
+
+        def ours():
+            _lib.check(L.cpw_b200_zgemm_i8(ctx.handle, ord(ta), m, n, k, C.c_void_p(a.data_ptr()), lda,
+                                           C.c_void_p(b.data_ptr()), k, 1.0, 0, C.c_void_p(c.data_ptr()), m,
+                                           args.slices, C.c_void_p(st)))
+
+        def theirs():
+            return (a.conj().t() if ta == "C" else a) @ b
+
+        res = {}
+        for name, fn in (("i8", ours), ("cublas", theirs)):
+            for _ in range(args.warmup):
+                fn()
+            torch.cuda.synchronize()
+            ts = []
+            for _ in range(args.steps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                fn()
+                e1.record()
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            ms = statistics.median(ts)
+            res[name] = {"ms": ms, "tflops_complex": 8.0 * m * n * k / (ms / 1e3) / 1e12}
+        ctx.synchronize()
+        ref = theirs()
+        res["rel_err"] = float((c - ref).abs().max() / ref.abs().max())
+        out["shapes"].append({"op": ta, "m": m, "n": n, "k": k, **res})
+        del a, b, c, ref
+        torch.cuda.empty_cache()
+    ctx.close()
+    print(json.dumps(out), flush=True)
+
+
 def run_profile(args, local):
     """Device path only, for ncu: --bands bands of the Si64 workload, --steps+--warmup calls."""
     import torch
@@ -699,7 +758,9 @@ def run_profile(args, local):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--mode", choices=["bench", "profile", "eig"], default="bench")
+    ap.add_argument("--mode", choices=["bench", "profile", "eig", "gemm"], default="bench")
+    ap.add_argument("--slices", type=int, default=7, help="gemm mode: int8 slices")
+    ap.add_argument("--nshapes", type=int, default=6, help="gemm mode: how many of the shapes")
     ap.add_argument("--workload", choices=["si216", "si64", "zb64"], default="si216", help="eig mode workload")
     ap.add_argument("--icmax", type=int, default=200, help="eig mode: outer iterations at most")
     ap.add_argument("--epspsi", type=float, default=1e-5, help="eig mode: residual tolerance")
@@ -728,6 +789,8 @@ def main():
             run_profile(args, local)
         elif args.mode == "eig":
             run_eig_study(args, local)
+        elif args.mode == "gemm":
+            run_gemm(args, local)
         elif args.impl == "reference":
             run_reference(args, rank)
         else:

@@ -31,6 +31,7 @@ SIGNATURES = {
     "cpw_b200_set_slab_budget": (I, [P, LL]),
     "cpw_b200_set_wait_limits": (I, [P, LL, LL]),
     "cpw_b200_wait_selftest": (I, [P, LL, P]),
+    "cpw_b200_set_projector_slices": (I, [P, I]),
     "cpw_b200_zgemm_i8": (I, [P, I, I, I, I, P, LL, P, LL, C.c_double, I, P, LL, I, P]),
     "cpw_b200_timing_begin": (I, [P]),
     "cpw_b200_timing_end": (I, [P, DP, C.POINTER(C.c_longlong), I]),
@@ -40,6 +41,8 @@ SIGNATURES = {
     "cpw_b200_set_projectors_device": (I, [P, I, P, I, P]),
     "cpw_b200_proj_nl_kb_device": (I, [P, DP, I, IP, DP, I, DP, IP, DP, DP, I, IP, I, DP, P, LL]),
     "cpw_b200_proj_nl_kb_der_device": (I, [P, I, DP, I, IP, DP, I, DP, IP, DP, DP, I, IP, I, DP, P, LL, LL, P, P]),
+    "cpw_b200_hamilt_kb_device": (I, [P, I, DP, IP, DP, I, IP, DP, DP, IP, IP, IP, DP, DP, DP, IP, DP, DP, IP, I, DP,
+                                      P, LL, I, I, I, I, I, I]),
     "cpw_b200_pot_local": (I, [P, DP, DP, DP, DP, DP, IP, I, I, IP, DP, DP, I, IP, I, I, I, I]),
     "cpw_b200_hk_psi_kin_device": (I, [P, I, P, LL, P, LL, I, I, P]),
     "cpw_b200_hk_psi_loc_c16_device": (I, [P, I, P, LL, P, LL, I, I, P]),

@@ -454,6 +454,14 @@ int cpw_b200_wait_selftest(cpw_b200_ctx* c, long long limit_ns, void* stream) {
   return tc_wait_selftest(c, (unsigned long long)limit_ns, stream ? (cudaStream_t)stream : c->stream);
 }
 
+int cpw_b200_set_projector_slices(cpw_b200_ctx* c, int slices) {
+  if (int s = check_ctx(c)) return s;
+  if (slices < 0 || slices > 8) return fail(kBadArg, "set_projector_slices: slices outside 0..8");
+  c->nl_slices = slices;
+  c->oz_nl_ready = false;
+  return kOk;
+}
+
 int cpw_b200_zgemm_i8(cpw_b200_ctx* c, int transa, int m, int n, int k, const void* a, long long lda, const void* b,
                       long long ldb, double alpha, int accumulate, void* cm, long long ldc, int slices, void* stream) {
   if (int s = check_ctx(c)) return s;
@@ -542,6 +550,18 @@ int cpw_b200_proj_nl_kb_der_device(cpw_b200_ctx* c, int nder, const double* rkpt
   cudaSetDevice(c->device);
   return ctx_proj_nl_kb_der(c, nder, rkpt, ntype, natom, rat, mxdatm, adot, nqnl, delqnl, vkb, mxdlqp, nkb, nanl,
                             xnlkb, anlga, ld, mxdanl, danlgadrk, d2anlgadrk2);
+}
+
+int cpw_b200_hamilt_kb_device(cpw_b200_ctx* c, int mtxd, const double* hdiag, const int* isort, const double* qmod,
+                              int ng, const int* kgv, const double* phase, const double* conj, const int* inds,
+                              const int* kmax, const int* indv, const double* ek, const double* sfact,
+                              const double* veff, const int* nqnl, const double* delqnl, const double* vkb,
+                              const int* nkb, int ntype, const double* adot, void* hamk, long long ldh, int mxdtyp,
+                              int mxdgve, int mxdnst, int mxdcub, int mxdlqp, int mxddim) {
+  if (int s = check_ctx(c)) return s;
+  cudaSetDevice(c->device);
+  return hamilt_kb_device(c, mtxd, hdiag, isort, qmod, ng, kgv, phase, conj, inds, kmax, indv, ek, sfact, veff, nqnl,
+                          delqnl, vkb, nkb, ntype, adot, hamk, ldh, mxdtyp, mxdgve, mxdnst, mxdcub, mxdlqp, mxddim);
 }
 
 int cpw_b200_pot_local(cpw_b200_ctx* c, double* vscr, double* vmax, double* vmin, double* cmax, const double* veff,

@@ -279,6 +279,7 @@ int ctx_set_projectors(cpw_b200_ctx* c, int nanl, const double* anlga, int ld, c
   e = cudaMemcpyAsync(c->xnl_h.data(), dx.p, nanl * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "set_projectors copy");
   c->tc_ready = false;
+  c->oz_nl_ready = false;
   e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "set_projectors");
   if (c->precision == 2) return tc_prepare_projectors(c);
@@ -310,7 +311,8 @@ int ctx_hkpsi_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, 
   // idle; Si216 28.5 -> 27.7 ms); the expansion follows the local kernels on st. The FP64 form
   // gains 0.5-1% this way and keeps both on st, so that its stage timers time each kernel alone.
   // CPW_B200_NL_OVERLAP=1 / 0 forces either way.
-  const bool cublas_nl = with_nl && c->nanl > 0 && !(c->precision == 2 && c->tc_ready);
+  const bool i8_nl = with_nl && c->nanl > 0 && c->nl_slices > 0;
+  const bool cublas_nl = with_nl && c->nanl > 0 && !i8_nl && !(c->precision == 2 && c->tc_ready);
   bool overlap = false;
   cudaEvent_t ov_t0 = nullptr, ov_t1 = nullptr;
   if (cublas_nl) {
@@ -396,6 +398,27 @@ int ctx_hkpsi_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, 
     cublasStatus_t bs;
     cudaEvent_t t0 = c->timer.on ? c->timer.take() : nullptr, t1 = c->timer.on ? c->timer.take() : nullptr;
     cudaEvent_t t2 = c->timer.on ? c->timer.take() : nullptr;
+    if (i8_nl) {
+      // projector products on the int8 tensor cores (oz.cu): X and X D split into int8 tiles once
+      // per projector set, psi and P per call
+      if (!c->oz_nl_ready || c->oz_x.s != c->nl_slices) {
+        if ((s = oz_prepare_a(c->oz_x, true, c->nanl, c->mtxd, c->anl.p, c->mtxd, c->nl_slices, st)) ||
+            (s = oz_prepare_a(c->oz_xd, false, c->mtxd, c->nanl, c->anld.p, c->mtxd, c->nl_slices, st)))
+          return s;
+        c->oz_nl_ready = true;
+      }
+      if (t0) cudaEventRecord(t0, st);
+      // P = X^H psi (hk_psi_nl_c16.f90:82); hpsi += (X D) P (:87-96)
+      if ((s = oz_gemm_prepared(c->ozs, c->oz_x, nb, psi, ldpsi, 1.0, false, c->proj.p, c->nanl, c->tcs.wait_ns, st)))
+        return s;
+      if (t1) cudaEventRecord(t1, st);
+      if ((s = oz_gemm_prepared(c->ozs, c->oz_xd, nb, c->proj.p, c->nanl, 1.0, true, hpsi, ldh, c->tcs.wait_ns, st)))
+        return s;
+      if (t2) cudaEventRecord(t2, st);
+      c->timer.mark(kStNlProj, t0, t1);
+      c->timer.mark(kStNlExpand, t1, t2);
+      return kOk;
+    }
     if (c->precision == 2 && c->tc_ready) {
       // opt-in mixed form: split-TF32 tensor-core products (nl_tc.cu)
       if ((s = tc_nl_apply(c, nb, psi, ldpsi, hpsi, ldh, st, t0, t1, t2))) return s;

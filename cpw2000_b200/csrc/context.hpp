@@ -74,11 +74,22 @@ struct TcScratch {
   unsigned long long wait_ns = 2000000000ull;   // hand-off wait limit of the tensor-core GEMMs
 };
 int tc_wait_selftest(cpw_b200_ctx* c, unsigned long long limit_ns, cudaStream_t st);
-// work space of the int8 tensor-core (Ozaki) complex GEMM and its sticky error flag
+// an A operand of the int8 tensor-core (Ozaki) complex GEMM split into int8 tiles with its row
+// scales (oz.cu); kept and reused for products with the same A
+struct OzOperand {
+  DevBuf tiles, e;
+  int M = 0, K = 0, s = 0, nkb = 0, tiles_m = 0;
+  bool conj = false, ready = false;
+};
+// work space of the int8 tensor-core GEMM and its sticky error flag
 struct OzScratch {
-  DevBuf a, b, ea, eb, sa, sb, part, err;
+  OzOperand aop;
+  DevBuf b, eb, part, err;
   bool err_init = false;
 };
+int oz_prepare_a(OzOperand& op, bool conjA, int M, int K, const void* A, long long lda, int slices, cudaStream_t st);
+int oz_gemm_prepared(OzScratch& w, const OzOperand& op, int N, const void* B, long long ldb, double alpha,
+                     bool accumulate, void* C, long long ldc, unsigned long long wait_ns, cudaStream_t st);
 // C = alpha op(A) B (+ C) with op(A) = A or A^H, complex128 column-major, FP64-accurate on the
 // int8 tensor cores with `slices` 7-bit slices per operand (oz.cu)
 int oz_zgemm(OzScratch& w, bool conjA, int M, int N, int K, const void* A, long long lda, const void* B, long long ldb,
@@ -145,6 +156,12 @@ struct cpw_b200_ctx {
   cpwb::DevBuf tc_a1, tc_a2, tc_ga, tc_gb;
   cpwb::TcScratch tcs;
   cpwb::OzScratch ozs;          // int8 tensor-core GEMMs of the eigensolver's basis products
+  // projector products on the int8 tensor cores: nl_slices > 0 slices per operand (0: the
+  // precision form's default), X (for X^H psi) and X D (for hpsi += X D P) split once per set
+  int nl_slices = 0;
+  cpwb::OzOperand oz_x, oz_xd;
+  cpwb::OzOperand oz_gs[3];     // eigensolver: converged block of a Gram-Schmidt call, split once
+  bool oz_nl_ready = false;
   long long tc_k1p = 0, tc_k2p = 0;     // K blocks (32 reals) of the projection and expansion operands
   bool tc_ready = false;
 
@@ -195,6 +212,12 @@ int ctx_proj_nl_kb_der(cpw_b200_ctx* c, int nder, const double* rkpt, int ntype,
                        int mxdatm, const double* adot, const int* nqnl, const double* delqnl, const double* vkb,
                        int mxdlqp, const int* nkb, int nanl, double* xnlkb_out, void* anlga, long long ld,
                        long long mxdanl, void* danlgadrk, void* d2anlgadrk2);
+int hamilt_kb_device(cpw_b200_ctx* c, int mtxd, const double* hdiag, const int* isort, const double* qmod, int ng,
+                     const int* kgv, const double* phase, const double* conj, const int* inds, const int* kmax,
+                     const int* indv, const double* ek, const double* sfact, const double* veff, const int* nqnl,
+                     const double* delqnl, const double* vkb, const int* nkb, int ntype, const double* adot,
+                     void* hamk, long long ldh, int mxdtyp, int mxdgve, int mxdnst, int mxdcub, int mxdlqp,
+                     int mxddim);
 int ctx_hkpsi_device(cpw_b200_ctx* c, int nb, const void* psi, long long ldpsi, void* hpsi, long long ldh,
                      cudaStream_t st, bool with_kinetic, bool with_nl);
 }  // namespace cpwb

@@ -375,6 +375,7 @@ struct Solver {
   // launches cost more than they save there)
   bool basis_i8 = false;
   int oz_slices = 7;
+
   long long n_i8 = 0, n_cublas = 0;
   static constexpr double kI8MinFlops = 2e9;
 
@@ -798,23 +799,51 @@ struct Solver {
       // leading columns with zero rows below zrows: their products run over zrows rows
       const int c0 = structured ? std::min(zcols, nconv) : 0;
       Z* y = x + (size_t)nconv * m;
+      const Z* xc = x + (size_t)c0 * m;
+      // on the int8 tensor cores the converged block is split once for both passes: as A^H for
+      // T = X^H Y, as A for Y -= X T (and H X for H Y -= H X T)
+      const bool i8 = basis_i8 && 8.0 * (nconv - c0) * k * m >= kI8MinFlops;
+      // (the splits live in the context: freeing device memory per call would synchronise the device)
+      OzOperand& x_cn = c->oz_gs[0];
+      OzOperand& x_nn = c->oz_gs[1];
+      OzOperand& hx_nn = c->oz_gs[2];
+      if (i8) {
+        ++n_i8;
+        if (int s = oz_prepare_a(x_cn, true, nconv - c0, m, xc, m, oz_slices, st)) return s;
+        if (int s = oz_prepare_a(x_nn, false, m, nconv - c0, xc, m, oz_slices, st)) return s;
+        if (also)
+          if (int s = oz_prepare_a(hx_nn, false, m, nconv, hx, m, oz_slices, st)) return s;
+      }
       for (int pass = 0; pass < 2; ++pass) {
         if (c0 > 0)
           if (int s = gemm(CUBLAS_OP_C, CUBLAS_OP_N, c0, k, zrows, one, x, m, y, m, zero, t, nconv, "grsch_loop t0"))
             return s;
-        if (int s = gemm(CUBLAS_OP_C, CUBLAS_OP_N, nconv - c0, k, m, one, x + (size_t)c0 * m, m, y, m, zero, t + c0,
-                         nconv, "grsch_loop t"))
-          return s;
-        if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_N, m, k, nconv - c0, mone, x + (size_t)c0 * m, m, t + c0, nconv, one,
-                         y, m, "grsch_loop x"))
-          return s;
+        if (i8) {
+          if (int s = oz_gemm_prepared(c->ozs, x_cn, k, y, m, 1.0, false, t + c0, nconv, c->tcs.wait_ns, st))
+            return s;
+          if (int s = oz_gemm_prepared(c->ozs, x_nn, k, t + c0, nconv, -1.0, true, y, m, c->tcs.wait_ns, st))
+            return s;
+        } else {
+          if (int s = gemm(CUBLAS_OP_C, CUBLAS_OP_N, nconv - c0, k, m, one, xc, m, y, m, zero, t + c0, nconv,
+                           "grsch_loop t"))
+            return s;
+          if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_N, m, k, nconv - c0, mone, xc, m, t + c0, nconv, one, y, m,
+                           "grsch_loop x"))
+            return s;
+        }
         if (c0 > 0)
           if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_N, zrows, k, c0, mone, x, m, t, nconv, one, y, m, "grsch_loop x0"))
             return s;
-        if (also)
-          if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_N, m, k, nconv, mone, hx, m, t, nconv, one, hx + (size_t)nconv * m,
-                           m, "grsch_loop hx"))
+        if (also) {
+          if (i8) {
+            if (int s = oz_gemm_prepared(c->ozs, hx_nn, k, t, nconv, -1.0, true, hx + (size_t)nconv * m, m,
+                                         c->tcs.wait_ns, st))
+              return s;
+          } else if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_N, m, k, nconv, mone, hx, m, t, nconv, one,
+                                  hx + (size_t)nconv * m, m, "grsch_loop hx")) {
             return s;
+          }
+        }
       }
     }
     if (chol) {

@@ -30,7 +30,7 @@
 //
 // Kernel (persistent; work item = 128 x 64 output tile x K range; 10 warps):
 //   warp 0      producer: per K block the s B' slice tiles (one stage of a 2-deep ring), then
-//               the s A' slice tiles one by one (3-deep ring of 16 KB stages); bulk copies
+//               the s A' slice tiles one by one (6-deep ring of 16 KB stages); bulk copies
 //               (cp.async.bulk, no tensor map, no multicast) completing on mbarriers;
 //   warp 1      allocates 512 TMEM columns (s groups x 64 columns of int32) and issues
 //               tcgen05.mma.cta_group::1.kind::i8 (M 128, N 64, K 32): for A' slice p, the B'
@@ -45,6 +45,7 @@
 #include <stdlib.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "context.hpp"
 
@@ -55,7 +56,7 @@ constexpr int BM = 128;                 // rows of D per tile
 constexpr int BN = 64;                  // real columns of D per tile (32 complex columns)
 constexpr int KBYTES = 128;             // int8 K elements per K block
 constexpr int kMaxSlices = 8;
-constexpr int kAStages = 3;
+constexpr int kAStages = 6;
 constexpr int kBStages = 2;
 constexpr int kATile = BM * KBYTES;     // 16 KB
 constexpr int kBTile = BN * KBYTES;     // 8 KB
@@ -73,8 +74,8 @@ inline size_t smem_bytes(int s) {
 struct Args {
   const int8_t* a;             // tiled A' slices: s x RBM x NKB tiles
   const int8_t* b;             // tiled B' slices: s x RBN x NKB tiles
-  const double* sa;            // 2^eA per row of A' (M)
-  const double* sb;            // 2^eB per column of B (N)
+  const int* ea;               // row exponents of A' (M)
+  const int* eb;               // column exponents of B (N)
   int M, N;                    // complex output dimensions (A' has M rows, B' has 2N rows)
   int s;                       // slices
   int nkb;                     // K blocks of K'
@@ -88,6 +89,15 @@ struct Args {
   int* err;
   unsigned long long wait_ns;
 };
+
+// row exponents not raised by any nonzero element (all-zero rows: scale 1)
+constexpr int kNoExp = (int)0x80808080;           // memset byte 0x80
+__device__ __forceinline__ int chunk_exp(double mx) {
+  int e = kNoExp;
+  if (mx > 0.0) frexp(mx, &e);
+  return e;
+}
+__device__ __forceinline__ int exp_or0(int e) { return e == kNoExp ? 0 : e; }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -380,13 +390,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_oz_gemm(const Args g) {
       // rows of this lane, 16 complex columns of this half
       const int i = w.m0 + 32 * quarter + lane;
       if (i < g.M) {
-        const double si = g.sa[i];
+        const int ei = exp_or0(g.ea[i]);
         const int j0 = (w.n0 + 32 * half) >> 1;
 #pragma unroll
         for (int c = 0; c < 16; ++c) {
           const int j = j0 + c;
           if (j < g.N) {
-            const double sc = si * g.sb[j];
+            const double sc = ldexp(1.0, ei + exp_or0(g.eb[j]));
             double re = acc[2 * c] * sc, im = acc[2 * c + 1] * sc;
             if (g.nsplit > 1) {
               g.part[((size_t)w.split * g.N + j) * g.M + i] = make_double2(re, im);
@@ -439,62 +449,61 @@ __global__ void k_oz_reduce(int M, int N, int nsplit, const double2* __restrict_
 
 // ---- splitting ----
 
-// 2^e with max |x| < 2^e (0 for an all-zero row)
-__device__ __forceinline__ int exp_of_max(double mx) {
-  int e = 0;
-  if (mx > 0.0) frexp(mx, &e);
-  return e;
-}
+// Row exponents: e with max |x| < 2^e over the row (frexp of the maximum). The reductions run in
+// parallel over K chunks and meet in an atomicMax of the exponent (the exponent of the maximum is
+// the maximum of the exponents); all-zero chunks leave the initial kNoExp (-> scale 1).
 
-// per column of a complex block (rows K, ld): scale 2^e of max(|re|, |im|); one warp per column
-__global__ void k_oz_scale_cols(int K, int ncol, const double2* __restrict__ x, long long ldx, int* __restrict__ e,
-                                double* __restrict__ sc) {
-  const int wpb = blockDim.x >> 5;
-  const int col = blockIdx.x * wpb + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (col >= ncol) return;
+constexpr int kExpChunk = 4096;                   // K elements per block of the column reduction
+
+// per column of a complex block (rows K, ld): grid (ncol, K chunks), 256 threads
+__global__ void __launch_bounds__(256) k_oz_exp_cols(int K, int ncol, const double2* __restrict__ x, long long ldx,
+                                                     int* __restrict__ e) {
+  const int col = blockIdx.x;
+  const int k0 = blockIdx.y * kExpChunk, k1 = min(K, k0 + kExpChunk);
   const double2* p = x + (size_t)col * ldx;
   double mx = 0.0;
-  for (int k = lane; k < K; k += 32) mx = fmax(mx, fmax(fabs(p[k].x), fabs(p[k].y)));
+  for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) mx = fmax(mx, fmax(fabs(p[k].x), fabs(p[k].y)));
   for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  if (lane == 0) {
-    const int ee = exp_of_max(mx);
-    e[col] = ee;
-    sc[col] = ldexp(1.0, ee);
+  __shared__ double wm[8];
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) mx = fmax(mx, wm[w]);
+    const int ce = chunk_exp(fmax(mx, wm[0]));
+    if (ce != kNoExp) atomicMax(&e[col], ce);
   }
 }
 
-// per row of a complex block (M rows, K columns, ld): one thread per row (coalesced across rows)
-__global__ void k_oz_scale_rows(int M, int K, const double2* __restrict__ x, long long ldx, int* __restrict__ e,
-                                double* __restrict__ sc) {
+constexpr int kExpRowChunk = 32;                  // K elements per thread of the row reduction
+
+// per row of a complex block (M rows, K columns, ld): thread per (row, K chunk), coalesced over rows
+__global__ void __launch_bounds__(256) k_oz_exp_rows(int M, int K, const double2* __restrict__ x, long long ldx,
+                                                     int* __restrict__ e) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= M) return;
+  const int k0 = blockIdx.y * kExpRowChunk, k1 = min(K, k0 + kExpRowChunk);
   double mx = 0.0;
-  for (int k = 0; k < K; ++k) {
+  for (int k = k0; k < k1; ++k) {
     const double2 v = x[(size_t)k * ldx + i];
     mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
   }
-  const int ee = exp_of_max(mx);
-  e[i] = ee;
-  sc[i] = ldexp(1.0, ee);
+  const int ce = chunk_exp(mx);
+  if (ce != kNoExp) atomicMax(&e[i], ce);
 }
 
-// the s digits of y in (-1, 1): y 2^6 = d_1 + d_2 2^-7 + ..., each |d| <= 64
-__device__ __forceinline__ void digits(double y, int s, int8_t* d) {
-  double v = y * 64.0;
-  for (int p = 0; p < s; ++p) {
-    const double r = rint(v);
-    d[p] = (int8_t)(int)r;
-    v = (v - r) * 128.0;
-  }
-}
+// The digits of y in (-1, 1): y 2^6 = d_1 + d_2 2^-7 + ..., each |d| <= 64, taken by rounding to
+// the nearest integer and scaling the exact remainder by 2^7 (the split kernels below).
 
 // byte offset of (row r, K byte k) inside a 128-byte-row swizzled tile
 __device__ __forceinline__ int swz(int r, int k) { return r * KBYTES + ((((k >> 4) ^ (r & 7)) << 4) | (k & 15)); }
 
 // A' slices. Row r of A': conjA ? column r of A (x(k, r) = A[k + r lda]) : row r (A[r + k lda]);
-// real K index 2k, 2k+1 = Re, Im of element k. One thread per (row, 16-byte chunk = 8 complex).
-__global__ void k_oz_split_a(int conjA, int M, int K, const double2* __restrict__ A, long long lda,
-                             const int* __restrict__ e, int s, int tiles_m, int nkb, int8_t* __restrict__ out) {
+// real K index 2k, 2k+1 = Re, Im of element k. One thread per (row, 16-byte chunk = 8 complex);
+// the slice count is a template parameter so that the digits stay in registers.
+template <int S>
+__global__ void __launch_bounds__(256) k_oz_split_a(int conjA, int M, int K, const double2* __restrict__ A,
+                                                    long long lda, const int* __restrict__ e, int tiles_m, int nkb,
+                                                    int8_t* __restrict__ out) {
   const long long nchunk = (long long)nkb * (KBYTES / 16);
   const long long total = (long long)tiles_m * BM * nchunk;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
@@ -510,33 +519,39 @@ __global__ void k_oz_split_a(int conjA, int M, int K, const double2* __restrict_
     if (r >= M) continue;
     const int kb = (int)(ch / (KBYTES / 16)), c16 = (int)(ch % (KBYTES / 16));
     const int k0 = (kb * KBYTES + c16 * 16) >> 1;          // first complex element of the chunk
-    const double scl = ldexp(1.0, -e[r]);
-    int8_t d[kMaxSlices][16];
+    const double scl = ldexp(1.0, -exp_or0(e[r]));
+    uint32_t w[S][4];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int k = k0 + u;
       double2 v = make_double2(0.0, 0.0);
       if (k < K) v = conjA ? A[(size_t)r * lda + k] : A[(size_t)k * lda + r];
-      int8_t dr[kMaxSlices], di[kMaxSlices];
-      digits(v.x * scl, s, dr);
-      digits(v.y * scl, s, di);
-      for (int p = 0; p < s; ++p) {
-        d[p][2 * u] = dr[p];
-        d[p][2 * u + 1] = di[p];
+      double vr = v.x * scl * 64.0, vi = v.y * scl * 64.0;
+#pragma unroll
+      for (int p = 0; p < S; ++p) {
+        const double dr = rint(vr), di = rint(vi);
+        const uint32_t pair = ((uint32_t)(uint8_t)(int8_t)(int)dr) | ((uint32_t)(uint8_t)(int8_t)(int)di << 8);
+        const int word = u >> 1, sh = (u & 1) * 16;
+        if (sh == 0) w[p][word] = pair; else w[p][word] |= pair << 16;
+        vr = (vr - dr) * 128.0;
+        vi = (vi - di) * 128.0;
       }
     }
     const int rb = r / BM, rr = r % BM;
-    for (int p = 0; p < s; ++p) {
+#pragma unroll
+    for (int p = 0; p < S; ++p) {
       int8_t* tile = out + (((size_t)p * tiles_m + rb) * nkb + kb) * kATile;
-      *reinterpret_cast<int4*>(tile + swz(rr, c16 * 16)) = *reinterpret_cast<const int4*>(d[p]);
+      *reinterpret_cast<uint4*>(tile + swz(rr, c16 * 16)) = make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
     }
   }
 }
 
 // B' slices: real rows 2j, 2j+1 from column j of B (conjA selects the pair of modes, see above).
-// One thread per (column, 16-byte chunk).
-__global__ void k_oz_split_b(int conjA, int N, int K, const double2* __restrict__ B, long long ldb,
-                             const int* __restrict__ e, int s, int tiles_n, int nkb, int8_t* __restrict__ out) {
+// One thread per (column, 16-byte chunk); the slice count is a template parameter.
+template <int S>
+__global__ void __launch_bounds__(256) k_oz_split_b(int conjA, int N, int K, const double2* __restrict__ B,
+                                                    long long ldb, const int* __restrict__ e, int tiles_n, int nkb,
+                                                    int8_t* __restrict__ out) {
   const long long nchunk = (long long)nkb * (KBYTES / 16);
   const long long total = (long long)N * nchunk;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
@@ -544,8 +559,8 @@ __global__ void k_oz_split_b(int conjA, int N, int K, const double2* __restrict_
     const long long ch = t % nchunk;
     const int kb = (int)(ch / (KBYTES / 16)), c16 = (int)(ch % (KBYTES / 16));
     const int k0 = (kb * KBYTES + c16 * 16) >> 1;
-    const double scl = ldexp(1.0, -e[j]);
-    int8_t d0[kMaxSlices][16], d1[kMaxSlices][16];
+    const double scl = ldexp(1.0, -exp_or0(e[j])) * 64.0;
+    uint32_t w0[S][4], w1[S][4];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int k = k0 + u;
@@ -553,28 +568,52 @@ __global__ void k_oz_split_b(int conjA, int N, int K, const double2* __restrict_
       if (k < K) v = B[(size_t)j * ldb + k];
       const double br = v.x * scl, bi = v.y * scl;
       // op(A) = A  : rows (br, -bi), (bi, br);  op(A) = A^H: rows (br, bi), (bi, -br)
-      const double r0a = br, r0b = conjA ? bi : -bi;
-      const double r1a = bi, r1b = conjA ? -br : br;
-      int8_t t0[kMaxSlices], t1[kMaxSlices], t2[kMaxSlices], t3[kMaxSlices];
-      digits(r0a, s, t0);
-      digits(r0b, s, t1);
-      digits(r1a, s, t2);
-      digits(r1b, s, t3);
-      for (int p = 0; p < s; ++p) {
-        d0[p][2 * u] = t0[p];
-        d0[p][2 * u + 1] = t1[p];
-        d1[p][2 * u] = t2[p];
-        d1[p][2 * u + 1] = t3[p];
+      double a0 = br, a1 = conjA ? bi : -bi, b0 = bi, b1 = conjA ? -br : br;
+#pragma unroll
+      for (int p = 0; p < S; ++p) {
+        const double d0 = rint(a0), d1 = rint(a1), d2 = rint(b0), d3 = rint(b1);
+        const uint32_t q0 = ((uint32_t)(uint8_t)(int8_t)(int)d0) | ((uint32_t)(uint8_t)(int8_t)(int)d1 << 8);
+        const uint32_t q1 = ((uint32_t)(uint8_t)(int8_t)(int)d2) | ((uint32_t)(uint8_t)(int8_t)(int)d3 << 8);
+        const int word = u >> 1, sh = (u & 1) * 16;
+        if (sh == 0) {
+          w0[p][word] = q0;
+          w1[p][word] = q1;
+        } else {
+          w0[p][word] |= q0 << 16;
+          w1[p][word] |= q1 << 16;
+        }
+        a0 = (a0 - d0) * 128.0;
+        a1 = (a1 - d1) * 128.0;
+        b0 = (b0 - d2) * 128.0;
+        b1 = (b1 - d3) * 128.0;
       }
     }
+#pragma unroll
     for (int row = 0; row < 2; ++row) {
       const int r = 2 * j + row;
       const int rb = r / BN, rr = r % BN;
-      for (int p = 0; p < s; ++p) {
+#pragma unroll
+      for (int p = 0; p < S; ++p) {
         int8_t* tile = out + (((size_t)p * tiles_n + rb) * nkb + kb) * kBTile;
-        *reinterpret_cast<int4*>(tile + swz(rr, c16 * 16)) = *reinterpret_cast<const int4*>(row ? d1[p] : d0[p]);
+        const uint4 q = row ? make_uint4(w1[p][0], w1[p][1], w1[p][2], w1[p][3])
+                            : make_uint4(w0[p][0], w0[p][1], w0[p][2], w0[p][3]);
+        *reinterpret_cast<uint4*>(tile + swz(rr, c16 * 16)) = q;
       }
     }
+  }
+}
+
+// run f with the slice count as a compile-time constant
+template <class F> void with_slices(int s, F f) {
+  switch (s) {
+    case 1: f(std::integral_constant<int, 1>{}); break;
+    case 2: f(std::integral_constant<int, 2>{}); break;
+    case 3: f(std::integral_constant<int, 3>{}); break;
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    case 5: f(std::integral_constant<int, 5>{}); break;
+    case 6: f(std::integral_constant<int, 6>{}); break;
+    case 7: f(std::integral_constant<int, 7>{}); break;
+    default: f(std::integral_constant<int, 8>{}); break;
   }
 }
 
@@ -584,13 +623,55 @@ int grid_for(long long work, int nsm) {
 
 }  // namespace oz
 
-// C = alpha op(A) B (+ C), complex128 column-major (see the head of this file)
-int oz_zgemm(OzScratch& w, bool conjA, int M, int N, int K, const void* A, long long lda, const void* B, long long ldb,
-             double alpha, bool accumulate, void* C, long long ldc, int slices, unsigned long long wait_ns,
-             cudaStream_t st) {
+// Split A' (op(A), M x K complex) into `slices` int8 tiles with its row scales; reusable by
+// every product with the same A (the projectors of a k-point).
+int oz_prepare_a(OzOperand& op, bool conjA, int M, int K, const void* A, long long lda, int slices, cudaStream_t st) {
   using namespace oz;
-  if (M <= 0 || N <= 0) return kOk;
+  op.ready = false;
   if (slices < 1 || slices > kMaxSlices) return fail(kBadArg, "oz_zgemm: slices outside 1..8");
+  op.M = M;
+  op.K = K;
+  op.s = slices;
+  op.conj = conjA;
+  if (M <= 0 || K <= 0) {
+    op.ready = true;
+    return kOk;
+  }
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  op.nkb = (int)((2LL * K + KBYTES - 1) / KBYTES);
+  op.tiles_m = (M + BM - 1) / BM;
+  int rs;
+  if ((rs = op.tiles.ensure((size_t)slices * op.tiles_m * op.nkb * kATile)) ||
+      (rs = op.e.ensure(sizeof(int) * (size_t)M)))
+    return rs;
+  const double2* a = (const double2*)A;
+  cudaError_t e0 = cudaMemsetAsync(op.e.p, 0x80, sizeof(int) * (size_t)M, st);
+  if (e0 != cudaSuccess) return cuda_fail(e0, "oz_zgemm");
+  if (conjA)
+    k_oz_exp_cols<<<dim3((unsigned)M, (unsigned)((K + kExpChunk - 1) / kExpChunk)), 256, 0, st>>>(K, M, a, lda,
+                                                                                               (int*)op.e.p);
+  else
+    k_oz_exp_rows<<<dim3((unsigned)((M + 255) / 256), (unsigned)((K + kExpRowChunk - 1) / kExpRowChunk)), 256, 0,
+                    st>>>(M, K, a, lda, (int*)op.e.p);
+  with_slices(slices, [&](auto sc) {
+    k_oz_split_a<decltype(sc)::value><<<grid_for((long long)op.tiles_m * BM * op.nkb * 8, nsm), 256, 0, st>>>(
+        conjA ? 1 : 0, M, K, a, lda, (const int*)op.e.p, op.tiles_m, op.nkb, (int8_t*)op.tiles.p);
+  });
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "oz_zgemm splitting");
+  op.ready = true;
+  return kOk;
+}
+
+// C = alpha op(A) B (+ C) with op(A) prepared by oz_prepare_a
+int oz_gemm_prepared(OzScratch& w, const OzOperand& op, int N, const void* B, long long ldb, double alpha,
+                     bool accumulate, void* C, long long ldc, unsigned long long wait_ns, cudaStream_t st) {
+  using namespace oz;
+  const int M = op.M, K = op.K, s = op.s;
+  if (M <= 0 || N <= 0) return kOk;
+  if (!op.ready) return fail(kNotReady, "oz_zgemm: operand not prepared");
   cudaError_t e;
   if (K <= 0) {
     if (!accumulate) {
@@ -602,43 +683,49 @@ int oz_zgemm(OzScratch& w, bool conjA, int M, int N, int K, const void* A, long 
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const int s = slices;
-  const int nkb = (int)((2LL * K + KBYTES - 1) / KBYTES);
-  const int tiles_m = (M + BM - 1) / BM, tiles_n = (2 * N + BN - 1) / BN;
-  // K splits: enough work items for every SM, every split at most kMaxKbPerItem K blocks
+  const int nkb = op.nkb, tiles_m = op.tiles_m;
+  const int tiles_n = (2 * N + BN - 1) / BN;
+  // K splits: every split at most kMaxKbPerItem K blocks; among those, the count whose waves of
+  // work items over the SMs finish first (waves x K blocks per item), fewer splits on ties
   const int tiles = tiles_m * tiles_n;
-  int nsplit = std::max(1, (nkb + kMaxKbPerItem - 1) / kMaxKbPerItem);
-  while (tiles * nsplit < nsm && nsplit * 8 <= nkb) ++nsplit;
+  const int nmin = std::max(1, (nkb + kMaxKbPerItem - 1) / kMaxKbPerItem);
+  int nsplit = nmin;
+  long long best = -1;
+  for (int ns = nmin; ns <= std::min(nkb, nmin + 96); ++ns) {
+    const long long kbps_t = (nkb + ns - 1) / ns;
+    const long long ns_eff = (nkb + kbps_t - 1) / kbps_t;
+    const long long waves = ((long long)tiles * ns_eff + nsm - 1) / nsm;
+    const long long cost = waves * (kbps_t + 4);        // + the drain and partial store of an item
+    if (best < 0 || cost < best) {
+      best = cost;
+      nsplit = (int)ns_eff;
+    }
+  }
   const int kbps = (nkb + nsplit - 1) / nsplit;
   nsplit = (nkb + kbps - 1) / kbps;
-  const size_t abytes = (size_t)s * tiles_m * nkb * kATile, bbytes = (size_t)s * tiles_n * nkb * kBTile;
+  const size_t bbytes = (size_t)s * tiles_n * nkb * kBTile;
   int rs;
-  if ((rs = w.a.ensure(abytes)) || (rs = w.b.ensure(bbytes)) || (rs = w.ea.ensure(sizeof(int) * (size_t)M)) ||
-      (rs = w.eb.ensure(sizeof(int) * (size_t)N)) || (rs = w.sa.ensure(sizeof(double) * (size_t)M)) ||
-      (rs = w.sb.ensure(sizeof(double) * (size_t)N)) || (rs = w.err.ensure(sizeof(int))))
+  if ((rs = w.b.ensure(bbytes)) || (rs = w.eb.ensure(sizeof(int) * (size_t)N)) || (rs = w.err.ensure(sizeof(int))))
     return rs;
   if (!w.err_init) {
     if ((e = cudaMemsetAsync(w.err.p, 0, sizeof(int), st)) != cudaSuccess) return cuda_fail(e, "oz_zgemm");
     w.err_init = true;
   }
   if (nsplit > 1 && (rs = w.part.ensure(16 * (size_t)nsplit * M * N))) return rs;
-  const double2* a = (const double2*)A;
   const double2* b = (const double2*)B;
-  if (conjA)
-    k_oz_scale_cols<<<(M + 7) / 8, 256, 0, st>>>(K, M, a, lda, (int*)w.ea.p, (double*)w.sa.p);
-  else
-    k_oz_scale_rows<<<(M + 255) / 256, 256, 0, st>>>(M, K, a, lda, (int*)w.ea.p, (double*)w.sa.p);
-  k_oz_scale_cols<<<(N + 7) / 8, 256, 0, st>>>(K, N, b, ldb, (int*)w.eb.p, (double*)w.sb.p);
-  k_oz_split_a<<<grid_for((long long)tiles_m * BM * nkb * 8, nsm), 256, 0, st>>>(
-      conjA ? 1 : 0, M, K, a, lda, (const int*)w.ea.p, s, tiles_m, nkb, (int8_t*)w.a.p);
-  k_oz_split_b<<<grid_for((long long)N * nkb * 8, nsm), 256, 0, st>>>(conjA ? 1 : 0, N, K, b, ldb, (const int*)w.eb.p,
-                                                                      s, tiles_n, nkb, (int8_t*)w.b.p);
+  if ((e = cudaMemsetAsync(w.eb.p, 0x80, sizeof(int) * (size_t)N, st)) != cudaSuccess) return cuda_fail(e, "oz_zgemm");
+  k_oz_exp_cols<<<dim3((unsigned)N, (unsigned)((K + kExpChunk - 1) / kExpChunk)), 256, 0, st>>>(K, N, b, ldb,
+                                                                                             (int*)w.eb.p);
+  with_slices(s, [&](auto sc) {
+    k_oz_split_b<decltype(sc)::value><<<grid_for((long long)N * nkb * 8, nsm), 256, 0, st>>>(
+        op.conj ? 1 : 0, N, K, b, ldb, (const int*)w.eb.p, tiles_n, nkb, (int8_t*)w.b.p);
+  });
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "oz_zgemm splitting");
   Args g{};
-  g.a = (const int8_t*)w.a.p;
+  g.a = (const int8_t*)op.tiles.p;
   g.b = (const int8_t*)w.b.p;
-  g.sa = (const double*)w.sa.p;
-  g.sb = (const double*)w.sb.p;
+  g.ea = (const int*)op.e.p;
+  g.eb = (const int*)w.eb.p;
   g.M = M;
   g.N = N;
   g.s = s;
@@ -655,8 +742,7 @@ int oz_zgemm(OzScratch& w, bool conjA, int M, int N, int K, const void* A, long 
   g.err = (int*)w.err.p;
   g.wait_ns = wait_ns;
   const size_t smem = smem_bytes(s);
-  if ((e = smem_limit((const void*)k_oz_gemm, (size_t)smem)) != cudaSuccess)
-    return cuda_fail(e, "oz_zgemm attribute");
+  if ((e = smem_limit((const void*)k_oz_gemm, smem)) != cudaSuccess) return cuda_fail(e, "oz_zgemm attribute");
   const int items = tiles * nsplit;
   k_oz_gemm<<<std::min(items, nsm), kThreads, smem, st>>>(g);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "oz_zgemm launch");
@@ -666,6 +752,15 @@ int oz_zgemm(OzScratch& w, bool conjA, int M, int N, int K, const void* A, long 
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "oz_zgemm reduce");
   }
   return kOk;
+}
+
+// C = alpha op(A) B (+ C), complex128 column-major (see the head of this file)
+int oz_zgemm(OzScratch& w, bool conjA, int M, int N, int K, const void* A, long long lda, const void* B, long long ldb,
+             double alpha, bool accumulate, void* C, long long ldc, int slices, unsigned long long wait_ns,
+             cudaStream_t st) {
+  if (M <= 0 || N <= 0) return kOk;
+  if (int s = oz_prepare_a(w.aop, conjA, M, K, A, lda, slices, st)) return s;
+  return oz_gemm_prepared(w, w.aop, N, B, ldb, alpha, accumulate, C, ldc, wait_ns, st);
 }
 
 int oz_read_error(OzScratch& w) {

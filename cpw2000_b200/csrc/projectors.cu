@@ -376,6 +376,7 @@ int ctx_proj_nl_kb(cpw_b200_ctx* c, const double* rkpt, int ntype, const int* na
   ProjGeom& g = T.g;
   c->nanl = nanl;
   c->tc_ready = false;
+  c->oz_nl_ready = false;
   if (xnlkb_out)
     for (int j = 0; j < nanl; ++j) xnlkb_out[j] = xnl[j];
   c->xnl_h = xnl;

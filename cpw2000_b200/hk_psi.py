@@ -144,6 +144,10 @@ class Context:
         """Limits of the bounded device waits (negative: the defaults, 2 s and 2^24 polls)."""
         check(self._L.cpw_b200_set_wait_limits(self.handle, int(mbarrier_ns), int(grid_polls)))
 
+    def set_projector_slices(self, slices: int):
+        """Projector products on the int8 tensor cores with that many slices (0: the form's default)."""
+        check(self._L.cpw_b200_set_projector_slices(self.handle, int(slices)))
+
     def set_slab_budget(self, nbytes: int):
         check(self._L.cpw_b200_set_slab_budget(self.handle, int(nbytes)))
 

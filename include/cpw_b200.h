@@ -89,6 +89,15 @@ int cpw_b200_set_slab_budget(cpw_b200_ctx* ctx, long long bytes);
 int cpw_b200_set_wait_limits(cpw_b200_ctx* ctx, long long mbarrier_ns, long long grid_polls);
 int cpw_b200_wait_selftest(cpw_b200_ctx* ctx, long long limit_ns, void* stream);
 
+/* Projector products P = X^H psi and hpsi += X D P (hk_psi_nl_c16.f90:82-96) of
+ * the context's H|psi> on the int8 tensor cores with `slices` 7-bit slices per
+ * operand (1..8; the split of X and X D is kept until the projectors change),
+ * in any precision form; 0 restores the form's default (cuBLAS FP64 ZGEMMs in
+ * FP64 and MIXED, split-TF32 tensor-core GEMMs in MIXED_TC). 7 slices give
+ * FP64-level products (~2^-48 of the row maxima); 4 give ~2^-27, without the
+ * bias of FP32 accumulation (the integer sums are exact). */
+int cpw_b200_set_projector_slices(cpw_b200_ctx* ctx, int slices);
+
 /* FP64-accurate complex GEMM on the int8 tensor cores (no counterpart in the
  * reference, whose ZGEMMs are BLAS calls): C = alpha op(A) B (+ C when
  * accumulate != 0), op(A) = A (transa 'N', A m x k) or A^H (transa 'C', A k x
@@ -150,6 +159,22 @@ int cpw_b200_proj_nl_kb_der_device(cpw_b200_ctx* ctx, int nder, const double* rk
                                    const double* delqnl, const double* vkb, int mxdlqp, const int* nkb, int nanl,
                                    double* xnlkb, void* anlga, long long ld, long long mxdanl, void* danlgadrk,
                                    void* d2anlgadrk2);
+
+/* The small dense Hamiltonian of the start basis on the device: replaces
+ * Src/ALFA/hamilt_kb.f90:1-234 (same arguments and layouts, host arrays:
+ * hdiag/isort/qmod (mtxd), kgv(3, mxdgve), phase(mxdgve) complex(8),
+ * conj(mxdgve), inds(mxdgve) 1-based stars, kmax(3), indv(mxdcub), ek(mxdnst),
+ * sfact(mxdtyp, mxdnst) complex(8), veff(mxdnst) complex(8), nqnl/delqnl
+ * (mxdtyp), vkb(-2:mxdlqp, 0:3, -1:1, mxdtyp), nkb(0:3, -1:1, mxdtyp), adot).
+ * hamk is a device complex128 array (ldh >= mtxd) that receives the full
+ * Hermitian matrix (the reference's output, both triangles), ready to be
+ * copied to the hamsm argument of the eigensolver. Synchronous. */
+int cpw_b200_hamilt_kb_device(cpw_b200_ctx* ctx, int mtxd, const double* hdiag, const int* isort, const double* qmod,
+                              int ng, const int* kgv, const double* phase, const double* conj, const int* inds,
+                              const int* kmax, const int* indv, const double* ek, const double* sfact,
+                              const double* veff, const int* nqnl, const double* delqnl, const double* vkb,
+                              const int* nkb, int ntype, const double* adot, void* hamk, long long ldh, int mxdtyp,
+                              int mxdgve, int mxdnst, int mxdcub, int mxdlqp, int mxddim);
 
 /* Screened local potential on the FFT mesh, computed on the device: replaces
  * Src/cpw_lib/pot_local.f90:1-190 (same arguments and array layouts, host

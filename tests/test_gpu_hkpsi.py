@@ -285,3 +285,47 @@ def test_dropin_pipelined_band_chunks(cuda, pinned):
                  d["kmscr"], anl, d["xnlkb"], d["nanl"], mxddim, mxdbnd, d["nanl"], d["ng"], d["vscr"].size)
     assert relerr(hpsi[:m, :nb], oracle_hpsi(d, psi[:m], nb)) < TOL64
     assert np.all(hpsi[m:, :] == 5.0 - 5.0j) and np.all(hpsi[:, nb:] == 5.0 - 5.0j)
+
+
+@pytest.mark.parametrize("wname,ik,nb", [("si2", 3, 7), ("small", 1, 5)])
+def test_projector_products_on_int8_tensor_cores(cuda, wname, ik, nb):
+    # FP64 context with 7-slice int8 projector products: within the FP64 tolerance of the
+    # oracle; MIXED_TC with 4 slices: within the FP32 local-part tolerance
+    import torch
+    w = configs.WORKLOADS[wname]()
+    d = configs.kpoint_inputs(w, ik)
+    psi = configs.random_psi(d["mtxd"], nb, 300 + ik)
+    ref = oracle_hpsi(d, psi, nb)
+    ctx = H.Context(0).setup(d)
+    ctx.set_projector_slices(7)
+    assert relerr(run_device(ctx, psi, torch, cuda), ref) < TOL64
+    ctx.set_projector_slices(0)
+    assert relerr(run_device(ctx, psi, torch, cuda), ref) < TOL64
+    ctx.close()
+    ctx = H.Context(0, precision=H.MIXED_TC).setup(d)
+    ctx.set_projector_slices(4)
+    assert relerr(run_device(ctx, psi, torch, cuda), ref) < TOL32
+    ctx.close()
+
+
+def test_int8_projector_term_si64(cuda):
+    # the projector term alone on the Si64 cell (256 projectors, 26,529 plane waves), 7 and 4
+    # slices against FP64: 1e-12 and 1e-7 of its maximum
+    import torch
+    w = configs.si64_cubic()
+    d = configs.kpoint_inputs(w, 0)
+    nb = 24
+    psi = configs.random_psi(d["mtxd"], nb, 31)
+    want = O.hk_psi_nl_c16(psi, np.zeros_like(psi), d["anlga"], d["xnlkb"], ladd=True)
+    for slices, tol in ((7, 1e-12), (4, 1e-7)):
+        ctx = H.Context(0).setup(d)
+        ctx.set_projector_slices(slices)
+        full = run_device(ctx, psi, torch, cuda)
+        ctx.set_projector_slices(0)
+        ctx.close()
+        ctx = H.Context(0).setup(d)
+        loc = run_device(ctx, psi, torch, cuda, local_only=True)
+        kin = np.asarray(d["ekpg"])[:, None] * psi
+        ctx.close()
+        got = full - loc - kin
+        assert relerr(got, want) < tol, (slices, relerr(got, want))
