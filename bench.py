@@ -733,23 +733,80 @@ def run_gemm(args, local):
         out["shapes"].append({"op": ta, "m": m, "n": n, "k": k, **res})
         del a, b, c, ref
         torch.cuda.empty_cache()
+    # the subspace eigensolve size of the Si216 Ritz steps: torch.linalg.eigh (cuSOLVER) for reference
+    n = 1160
+    x = torch.randn((n, n), dtype=torch.complex128, device=dev)
+    hm = x + x.conj().t()
+    for _ in range(2):
+        torch.linalg.eigh(hm)
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.linalg.eigh(hm)
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    out["eigh_1160_ms"] = statistics.median(ts)
     ctx.close()
     print(json.dumps(out), flush=True)
 
 
+def run_tte(args, local):
+    """time_to_eigvals alone (the bench line's key of that name), for studies of the eigensolver."""
+    import torch
+    torch.cuda.set_device(local)
+    w = configs.si216_cubic()
+    nk = max(1, min(args.eig_kpoints, len(w.kpoints)))
+    inputs = [configs.kpoint_inputs(w, k, with_hamsm=True) for k in range(nk)]
+    out = time_to_eigvals(w, inputs, local, repeats=args.eig_repeats, workers=min(args.eig_workers, nk),
+                          budget_s=args.eig_budget)
+    print(json.dumps({"mode": "tte", **out}), flush=True)
+
+
+def run_eig_profile(args, local):
+    """One eigensolver run on the Si216 Gamma point in one precision form (--precision), --icmax
+    outer iterations, for ncu launch lists of the eigensolver's kernels."""
+    import torch
+
+    from cpw2000_b200 import ditsp as E
+    from cpw2000_b200 import hk_psi as H
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    d = configs.kpoint_inputs(configs.si216_cubic(), 0, with_hamsm=True)
+    nb = 480
+    prec = {"fp64": H.FP64, "mixed": H.MIXED, "mixed_tc": H.MIXED_TC}[args.precision]
+    ctx = H.Context(local, precision=prec).setup(d)
+    ctx.set_slab_budget(8 << 30)
+    P = torch.zeros((3 * nb, d["mtxd"]), dtype=torch.complex128, device=dev).t()
+    HP = torch.zeros_like(P)
+    t0 = time.perf_counter()
+    r = E.eigensolve(ctx, P, HP, nb, d["mtxds"], d["hamsm"], d["hdiag"], epspsi=1e-5, icmax=args.icmax,
+                     ipr=args.ipr)
+    torch.cuda.synchronize()
+    print(json.dumps({"mode": "eigprof", "precision": args.precision, "icmax": args.icmax,
+                      "seconds": time.perf_counter() - t0, "ihkpsum": r["ihkpsum"]}), flush=True)
+    ctx.close()
+
+
 def run_profile(args, local):
-    """Device path only, for ncu: --bands bands of the Si64 workload, --steps+--warmup calls."""
+    """Device path only, for ncu: --bands bands of the --pworkload workload (Si216 or Si64, Gamma),
+    --steps + --warmup calls."""
     import torch
 
     from cpw2000_b200 import hk_psi as H
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    d = configs.kpoint_inputs(configs.si64_cubic(), 0)
+    w = {"si216": configs.si216_cubic, "si64": configs.si64_cubic}[args.pworkload]()
+    d = configs.kpoint_inputs(w, 0)
     nb = args.bands
     psi = torch.from_numpy(np.ascontiguousarray(configs.random_psi(d["mtxd"], nb, 5).T)).to(dev).t()
     hpsi = torch.empty((nb, d["mtxd"]), dtype=torch.complex128, device=dev).t()
     ctx = H.Context(local, precision={"fp64": H.FP64, "mixed": H.MIXED, "mixed_tc": H.MIXED_TC}[args.precision]).setup(d)
-    ctx.set_slab_budget(4 << 30)
+    ctx.set_slab_budget(8 << 30)
+    if args.nl_slices:
+        ctx.set_projector_slices(args.nl_slices)
     for _ in range(args.warmup + args.steps):
         ctx.hk_psi(psi, hpsi)
     torch.cuda.synchronize()
@@ -758,7 +815,7 @@ def run_profile(args, local):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--mode", choices=["bench", "profile", "eig", "gemm"], default="bench")
+    ap.add_argument("--mode", choices=["bench", "profile", "eig", "gemm", "eigprof", "tte"], default="bench")
     ap.add_argument("--slices", type=int, default=7, help="gemm mode: int8 slices")
     ap.add_argument("--nshapes", type=int, default=6, help="gemm mode: how many of the shapes")
     ap.add_argument("--workload", choices=["si216", "si64", "zb64"], default="si216", help="eig mode workload")
@@ -772,6 +829,8 @@ def main():
     ap.add_argument("--ipr", type=int, default=0, help="eig mode: eigensolver print level (2: phase timers)")
     ap.add_argument("--save-traces", default="", help="eig mode: directory for the iteration traces (.npy)")
     ap.add_argument("--bands", type=int, default=NB, help="profile mode: bands per call")
+    ap.add_argument("--pworkload", choices=["si216", "si64"], default="si216", help="profile mode workload")
+    ap.add_argument("--nl-slices", type=int, default=0, help="profile mode: int8 projector slices (0: form default)")
     ap.add_argument("--precision", choices=["fp64", "mixed", "mixed_tc"], default="fp64", help="profile mode precision")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -791,6 +850,10 @@ def main():
             run_eig_study(args, local)
         elif args.mode == "gemm":
             run_gemm(args, local)
+        elif args.mode == "eigprof":
+            run_eig_profile(args, local)
+        elif args.mode == "tte":
+            run_tte(args, local)
         elif args.impl == "reference":
             run_reference(args, rank)
         else:

@@ -766,14 +766,17 @@ int tc_nl_apply_ops(TcScratch& t, int m, int na, long long nkb1, long long nkb2,
   if (t0) cudaEventRecord(t0, st);
   tc::k_split_psi<<<grid_for((long long)nb * nkb1 * 16, nsm), 256, 0, st>>>(nb, m, nkb1, (const C2<double>*)psi, ldpsi,
                                                                              b1, b1 + fb1);
-  tc::k_gemm_tf32x3<0><<<std::min(items1, nsm), tc::kThreads, tc::kSmemBytes, st>>>(g1);
+  // one CTA per work item: the hardware places CTAs on whichever SMs are free, so a GEMM that
+  // shares the GPU with other contexts' kernels is not held up by a few late CTAs of a fixed
+  // round-robin assignment
+  tc::k_gemm_tf32x3<0><<<items1, tc::kThreads, tc::kSmemBytes, st>>>(g1);
   if ((2LL * na) % tc::BK) {
     if ((e = cudaMemsetAsync(b2, 0, sizeof(float) * 2 * fb2, st)) != cudaSuccess) return cuda_fail(e, "tc nl");
   }
   tc::k_reduce_p<<<grid_for((long long)na * nb, nsm), 256, 0, st>>>(na, nb, nsplit, nkb2, (const double*)t.part.p,
                                                                     b2, b2 + fb2);
   if (t1) cudaEventRecord(t1, st);
-  tc::k_gemm_tf32x3<1><<<std::min(items2, nsm), tc::kThreads, tc::kSmemBytes, st>>>(g2);
+  tc::k_gemm_tf32x3<1><<<items2, tc::kThreads, tc::kSmemBytes, st>>>(g2);
   if (t2) cudaEventRecord(t2, st);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "tensor-core projector GEMMs");
   return kOk;
@@ -833,7 +836,7 @@ int tc_zgemm_nn(cpw_b200_ctx* c, int m, int n, int kk, const void* a, long long 
   g.wait_ns = c->tcs.wait_ns;
   if ((e = smem_limit((const void*)tc::k_gemm_tf32x3<1>, (size_t)tc::kSmemBytes)) != cudaSuccess)
     return cuda_fail(e, "tensor-core GEMM attribute");
-  tc::k_gemm_tf32x3<1><<<std::min(mt * nt, nsm), tc::kThreads, tc::kSmemBytes, st>>>(g);
+  tc::k_gemm_tf32x3<1><<<mt * nt, tc::kThreads, tc::kSmemBytes, st>>>(g);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "tensor-core zgemm");
   return kOk;
 }

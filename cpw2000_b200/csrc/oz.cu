@@ -28,9 +28,9 @@
 // K-major order the tensor cores read (row r at r * 128 bytes, 16-byte chunk c at
 // (c ^ (r & 7)) * 16): tile (p, row block, K block) at ((p * RB + rb) * NKB + kb) * tile bytes.
 //
-// Kernel (persistent; work item = 128 x 64 output tile x K range; 10 warps):
+// Kernel (one CTA per work item = 128 x 64 output tile x K range; 10 warps):
 //   warp 0      producer: per K block the s B' slice tiles (one stage of a 2-deep ring), then
-//               the s A' slice tiles one by one (6-deep ring of 16 KB stages); bulk copies
+//               the s A' slice tiles two by two (3-deep ring of 32 KB stages); bulk copies
 //               (cp.async.bulk, no tensor map, no multicast) completing on mbarriers;
 //   warp 1      allocates 512 TMEM columns (s groups x 64 columns of int32) and issues
 //               tcgen05.mma.cta_group::1.kind::i8 (M 128, N 64, K 32): for A' slice p, the B'
@@ -56,7 +56,8 @@ constexpr int BM = 128;                 // rows of D per tile
 constexpr int BN = 64;                  // real columns of D per tile (32 complex columns)
 constexpr int KBYTES = 128;             // int8 K elements per K block
 constexpr int kMaxSlices = 8;
-constexpr int kAStages = 6;
+constexpr int kAStages = 3;
+constexpr int kAPer = 2;                // A' slice tiles per stage
 constexpr int kBStages = 2;
 constexpr int kATile = BM * KBYTES;     // 16 KB
 constexpr int kBTile = BN * KBYTES;     // 8 KB
@@ -68,7 +69,7 @@ constexpr int kBarBytes = 256;
 constexpr unsigned long long kWaitNs = 2000000000ull;
 
 inline size_t smem_bytes(int s) {
-  return 1024 + (size_t)kAStages * kATile + (size_t)kBStages * s * kBTile + kBarBytes;
+  return 1024 + (size_t)kAStages * kAPer * kATile + (size_t)kBStages * s * kBTile + kBarBytes;
 }
 
 struct Args {
@@ -205,8 +206,8 @@ __device__ __forceinline__ Item item_of(const Args& g, int it) {
 __global__ void __launch_bounds__(kThreads, 1) k_oz_gemm(const Args g) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  unsigned char* aring = base;                                  // kAStages x 16 KB
-  unsigned char* bring = base + kAStages * kATile;              // kBStages x s x 8 KB
+  unsigned char* aring = base;                                  // kAStages x kAPer x 16 KB
+  unsigned char* bring = base + kAStages * kAPer * kATile;      // kBStages x s x 8 KB
   const int s = g.s;
   const size_t bslot = (size_t)s * kBTile;
   uint64_t* bars = reinterpret_cast<uint64_t*>(bring + kBStages * bslot);
@@ -273,8 +274,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_oz_gemm(const Args g) {
             }
             ++gb;
           }
-          // then the A' slice tiles one by one
-          for (int p = 0; p < s; ++p) {
+          // then the A' slice tiles, kAPer per stage
+          for (int p0 = 0; p0 < s; p0 += kAPer) {
             const int sa = (int)(ga % kAStages);
             const long long r = ga / kAStages;
             if (r > 0 && !mbar_wait(smem_u32(&a_empty[sa]), (uint32_t)((r - 1) & 1), &failed, g.wait_ns)) {
@@ -282,10 +283,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_oz_gemm(const Args g) {
               atomicExch(g.err, 1);
               break;
             }
+            const int np = min(kAPer, s - p0);
             const uint32_t fa = smem_u32(&a_full[sa]);
-            mbar_expect_tx(fa, bytes_a);
-            const int8_t* src = g.a + (((size_t)p * g.tiles_m + w.mt) * nkb + kb) * kATile;
-            bulk_load(smem_u32(aring + (size_t)sa * kATile), src, bytes_a, fa);
+            mbar_expect_tx(fa, (uint32_t)np * bytes_a);
+            for (int u = 0; u < np; ++u) {
+              const int8_t* src = g.a + (((size_t)(p0 + u) * g.tiles_m + w.mt) * nkb + kb) * kATile;
+              bulk_load(smem_u32(aring + ((size_t)sa * kAPer + u) * kATile), src, bytes_a, fa);
+            }
             ++ga;
           }
         }
@@ -320,22 +324,28 @@ __global__ void __launch_bounds__(kThreads, 1) k_oz_gemm(const Args g) {
             break;
           }
           asm volatile("tcgen05.fence::after_thread_sync;\n");
-          const uint32_t bbase = smem_u32(bring + sb * bslot);
-          for (int p = 0; p < s; ++p) {
+          // descriptors: the start-address field is the byte address / 16, so moving by q tiles and
+          // ks 32-byte K steps adds (q kBTile + 32 ks) / 16 to it
+          const uint64_t db = smem_desc(smem_u32(bring + sb * bslot));
+          for (int p0 = 0; p0 < s && ok; p0 += kAPer) {
             const int sa = (int)(ga % kAStages);
             if (!mbar_wait(smem_u32(&a_full[sa]), (uint32_t)((ga / kAStages) & 1), &failed, g.wait_ns)) {
               ok = false;
               break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n");
-            const uint32_t abase = smem_u32(aring + (size_t)sa * kATile);
-            for (int q = 0; q + p < s; ++q) {
-              const uint32_t tacc = tmem + (uint32_t)((p + q) * BN);
+            const int np = min(kAPer, s - p0);
+            for (int u = 0; u < np; ++u) {
+              const int p = p0 + u;
+              const uint64_t da = smem_desc(smem_u32(aring + ((size_t)sa * kAPer + u) * kATile));
+              for (int q = 0; q + p < s; ++q) {
+                const uint32_t tacc = tmem + (uint32_t)((p + q) * BN);
 #pragma unroll
-              for (int ks = 0; ks < KBYTES / 32; ++ks) {
-                // the first product of group p + q in this work item starts the accumulator
-                const uint32_t acc = (i == 0 && p == 0 && ks == 0) ? 0u : 1u;
-                mma_i8(tacc, smem_desc(abase + ks * 32), smem_desc(bbase + q * kBTile + ks * 32), idesc, acc);
+                for (int ks = 0; ks < KBYTES / 32; ++ks) {
+                  // the first product of group p + q in this work item starts the accumulator
+                  const uint32_t acc = (i == 0 && p == 0 && ks == 0) ? 0u : 1u;
+                  mma_i8(tacc, da + (uint64_t)(2 * ks), db + (uint64_t)(q * (kBTile >> 4) + 2 * ks), idesc, acc);
+                }
               }
             }
             mma_commit(smem_u32(&a_empty[sa]));
@@ -374,14 +384,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_oz_gemm(const Args g) {
       if (w.nblk > 0) {
         for (int grp = 0; grp < s; ++grp) {
           const double wgt = ldexp(1.0, -12 - 7 * grp);
+          uint32_t r[4][8];
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            uint32_t r[8];
-            tmem_ld8(lane_base + (uint32_t)(grp * BN + 32 * half + 8 * j), r);
-            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+          for (int j = 0; j < 4; ++j) tmem_ld8(lane_base + (uint32_t)(grp * BN + 32 * half + 8 * j), r[j]);
+          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-            for (int t = 0; t < 8; ++t) acc[8 * j + t] += (double)(int)r[t] * wgt;
-          }
+          for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int t = 0; t < 8; ++t) acc[8 * j + t] += (double)(int)r[j][t] * wgt;
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;\n");
@@ -744,7 +754,10 @@ int oz_gemm_prepared(OzScratch& w, const OzOperand& op, int N, const void* B, lo
   const size_t smem = smem_bytes(s);
   if ((e = smem_limit((const void*)k_oz_gemm, smem)) != cudaSuccess) return cuda_fail(e, "oz_zgemm attribute");
   const int items = tiles * nsplit;
-  k_oz_gemm<<<std::min(items, nsm), kThreads, smem, st>>>(g);
+  // one CTA per work item: the hardware places CTAs on whichever SMs are free, so a GEMM that
+  // shares the GPU with other contexts' kernels is not held up by a few late CTAs of a fixed
+  // round-robin assignment (the kernel still loops when given fewer CTAs than items)
+  k_oz_gemm<<<items, kThreads, smem, st>>>(g);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "oz_zgemm launch");
   if (nsplit > 1) {
     k_oz_reduce<<<grid_for((long long)M * N, nsm), 256, 0, st>>>(M, N, nsplit, (const double2*)w.part.p, alpha,

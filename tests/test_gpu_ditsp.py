@@ -31,14 +31,15 @@ def oracle_solve(d, nb, epspsi):
                        mxdbnd=3 * nb)
 
 
-def device_solve(d, nb, epspsi, prec, torch, dev, iguess=0, psi0=None):
+def device_solve(d, nb, epspsi, prec, torch, dev, iguess=0, psi0=None, icmax=40):
     ctx = H.Context(0, precision=prec).setup(d)
     m = d["mtxd"]
     psi = torch.zeros((3 * nb, m), dtype=torch.complex128, device=dev).t()
     if psi0 is not None:
         psi[:, : psi0.shape[1]] = torch.from_numpy(psi0).to(dev)
     hpsi = torch.zeros_like(psi)
-    r = E.eigensolve(ctx, psi, hpsi, nb, d["mtxds"], d["hamsm"], d["hdiag"], epspsi=epspsi, iguess=iguess)
+    r = E.eigensolve(ctx, psi, hpsi, nb, d["mtxds"], d["hamsm"], d["hdiag"], epspsi=epspsi, iguess=iguess,
+                     icmax=icmax)
     torch.cuda.synchronize()
     return r, psi.cpu().numpy(), hpsi.cpu().numpy()
 
@@ -124,3 +125,25 @@ def test_ditsp_full_diagonalisation_path(cuda):
     assert d["mtxds"] == d["mtxd"]
     r, psi, _ = device_solve(d, 6, 1e-5, H.FP64, torch, cuda)
     assert np.abs(r["ei"] - dense_eigs(d)[:6]).max() < 1e-12
+
+
+@pytest.fixture(scope="module")
+def c3_truth():
+    # one k-point of the batched-k-point cell (Si8 cubic, Ecut 20 Ha, 40^3 box, ~4,600 plane
+    # waves): the dense matrix of the operator, diagonalised on the CPU
+    w = configs.si8_cubic_kbatch(nk=4)
+    d = configs.kpoint_inputs(w, 1, with_hamsm=True)
+    return d, dense_eigs(d)
+
+
+@pytest.mark.parametrize("prec,tol", [(H.FP64, 1e-8), (H.MIXED_TC, 1e-6)])
+def test_ditsp_c3_kpoint_matches_dense_truth(cuda, c3_truth, prec, tol):
+    import torch
+    d, ev = c3_truth
+    nb = 40
+    assert d["mtxd"] > 4500
+    r, psi, hpsi = device_solve(d, nb, 1e-5, prec, torch, cuda, icmax=150)
+    err = np.abs(r["ei"] - ev[: r["neig"]]).max()
+    assert err < tol, f"max |e - e_dense| = {err:.3e} Ha"
+    if prec == H.FP64:
+        assert r["converged"] and D.ditsp_error(psi[:, : r["neig"]], hpsi[:, : r["neig"]]) < 1e-10
