@@ -42,6 +42,11 @@ StageTimer::~StageTimer() {
 
 int DevBuf::ensure(size_t need) {
   if (need <= bytes && p) return kOk;
+  // a buffer that grows takes 1.5x (at least) of its old size, rounded to 2 MiB: buffers sized by
+  // the eigensolver's growing blocks are then reallocated a few times per solve instead of every
+  // iteration (cudaFree synchronises the whole device, stalling every context that shares it)
+  if (p) need = std::max(need, bytes + bytes / 2);
+  if (need > (1u << 20)) need = (need + (2u << 20) - 1) & ~(size_t)((2u << 20) - 1);
   release();
   if (need == 0) return kOk;
   cudaError_t e = cudaMalloc(&p, need);
