@@ -14,7 +14,10 @@
  * 4, 5 butterflies, generic O(p^2) for other primes), standing in for the
  * FFTPACK backend of Src/fft/_ncar (any exact FFT gives the same result to
  * rounding). The GEMMs are plain OpenMP loops, like the vendored netlib BLAS
- * of Src/LIBS/blas that the reference links when COMPBLAS=true.
+ * of Src/LIBS/blas that the reference links when COMPBLAS=true, unless an
+ * optimised cblas_zgemm is handed in with cpw_ref_set_zgemm (the reference's
+ * default build, COMPBLAS=false at Src/config/make.inc:95, links an external
+ * optimised BLAS).
  *
  * Build: see oracle/Makefile (gcc -O3 -fopenmp -shared).
  */
@@ -201,6 +204,14 @@ static void cfft_wf(box_t* B, cplx* chd, int mode) {
   }
 }
 
+/* an optimised complex GEMM with the 64-bit-integer CBLAS interface (column-major) */
+typedef void (*zgemm64_fn)(int order, int transa, int transb, long long m, long long n, long long k,
+                           const void* alpha, const void* a, long long lda, const void* b, long long ldb,
+                           const void* beta, void* c, long long ldc);
+static zgemm64_fn g_zgemm = NULL;
+void cpw_ref_set_zgemm(void* fn) { g_zgemm = (zgemm64_fn)fn; }
+int cpw_ref_has_zgemm(void) { return g_zgemm != NULL; }
+
 int cpw_ref_max_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();
@@ -245,6 +256,17 @@ int cpw_ref_hk_psi(int mtxd, int neig, const cplx* psi, int ld, cplx* hpsi, int 
   if (nanl > 0 && neig > 0) {
     cplx* dhd = (cplx*)malloc(sizeof(cplx) * (size_t)nanl * neig);
     if (!dhd) return -1;
+    if (g_zgemm) {
+      /* the two ZGEMMs of hk_psi_nl_c16.f90:82 and :95 in the optimised BLAS (CblasColMajor 102,
+         CblasNoTrans 111, CblasConjTrans 113) */
+      const cplx one = 1.0, zero = 0.0;
+      g_zgemm(102, 113, 111, nanl, neig, mtxd, &one, anlga, lda, psi, ld, &zero, dhd, nanl);
+      for (int n = 0; n < neig; ++n)
+        for (int a = 0; a < nanl; ++a) dhd[(size_t)n * nanl + a] *= xnlkb[a];
+      g_zgemm(102, 111, 111, mtxd, neig, nanl, &one, anlga, lda, dhd, nanl, &one, hpsi, ldh);
+      free(dhd);
+      return 0;
+    }
     /* dhd = anlga^H psi ; dhd = diag(xnlkb) dhd */
 #pragma omp parallel for collapse(2) schedule(static)
     for (int n = 0; n < neig; ++n)

@@ -22,6 +22,18 @@ def build():
     return SO
 
 
+_blas = None
+
+
+def openblas_path():
+    """numpy's bundled OpenBLAS (64-bit integers, scipy_ prefixed symbols), or None."""
+    import glob
+
+    import numpy
+    hits = glob.glob(os.path.join(os.path.dirname(numpy.__file__), "..", "numpy.libs", "*openblas64*.so*"))
+    return hits[0] if hits else None
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -30,8 +42,30 @@ def lib():
         L = C.CDLL(SO)
         L.cpw_ref_hk_psi.restype = C.c_int
         L.cpw_ref_max_threads.restype = C.c_int
+        L.cpw_ref_has_zgemm.restype = C.c_int
+        L.cpw_ref_set_zgemm.argtypes = [C.c_void_p]
         _lib = L
     return _lib
+
+
+def use_blas(on: bool = True) -> bool:
+    """Projector ZGEMMs of the restatement in numpy's OpenBLAS (on) or in its own loops (off).
+    Returns whether the optimised GEMM is in use."""
+    global _blas
+    L = lib()
+    if not on:
+        L.cpw_ref_set_zgemm(None)
+        return False
+    if _blas is None:
+        path = openblas_path()
+        if path is None:
+            return False
+        _blas = C.CDLL(path)
+    fn = getattr(_blas, "scipy_cblas_zgemm64_", None)
+    if fn is None:
+        return False
+    L.cpw_ref_set_zgemm(C.cast(fn, C.c_void_p))
+    return bool(L.cpw_ref_has_zgemm())
 
 
 def max_threads() -> int:

@@ -4,7 +4,8 @@ baseline of the bench) against the numpy restatement (oracle/hk_psi.py).
 Both restate Src/hk_psi/reference/hk_psi_c16.f90:28-241; they differ only in FFT
 algorithm and summation order, so they agree to rounding (<= 1e-12 of max|H psi|),
 on the Si2 fcc cell (32^3 box) and on a triclinic cell with a non-cubic box
-(24 x 20 x 18, leading dimension id = 25), with 1 and with several threads.
+(24 x 20 x 18, leading dimension id = 25), with 1 and with several threads, with the
+projector products in its own loops and in numpy's bundled OpenBLAS zgemm.
 """
 import numpy as np
 import pytest
@@ -38,3 +39,15 @@ def test_c_restatement_box_is_not_cubic():
     d = configs.kpoint_inputs(configs.WORKLOADS["small"](), 1)
     n1, n2, n3, ident = (int(v) for v in d["kmscr"][3:7])
     assert len({n1, n2, n3}) == 3 and ident > n1
+
+
+@pytest.mark.parametrize("wname,ik,nb", [("si2", 2, 5), ("small", 1, 4)])
+def test_c_restatement_with_optimised_blas(wname, ik, nb):
+    if not c_ref.use_blas(True):
+        pytest.skip("numpy ships no 64-bit-integer OpenBLAS here")
+    try:
+        ref, got, _ = _both(wname, ik, nb, 70 + ik, 2)
+    finally:
+        c_ref.use_blas(False)
+    err = float(np.abs(got - ref).max() / np.abs(ref).max())
+    assert err < TOL64, f"{wname} k{ik}: relative difference {err:.3e}"
