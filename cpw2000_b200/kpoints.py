@@ -24,7 +24,7 @@ from .hk_psi import FP64, Context
 
 def eigensolve_kpoints(inputs: list[dict], nbands: int, workers: int = 8, precision: int = FP64, epspsi=1e-5,
                        icmax=60, device: int = 0, seed: int = 0, mxdbnd: int | None = None, trace: bool = False,
-                       keep: int = 0, slab_budget: int = 0, env: dict | None = None):
+                       keep: int = 0, slab_budget: int = 0, env: dict | None = None, ipr: int = 0):
     """Run ditsp for every k-point dict of ``inputs`` (configs.kpoint_inputs(..., with_hamsm=True)).
 
     Returns (results, seconds): results[k] = dict(ei, neig, ihkpsum, converged) in input order,
@@ -34,6 +34,7 @@ def eigensolve_kpoints(inputs: list[dict], nbands: int, workers: int = 8, precis
     times from the common start of the set. keep: the first ``keep`` columns of each k-point's
     converged psi are returned (device tensors, ``psi``). slab_budget: FFT slab bytes per context.
     env: environment variables set while the set runs (the eigensolver reads its switches then).
+    ipr: the eigensolver's print level (2: per-phase wall times of every k-point).
     """
     import torch
     dev = torch.device("cuda", device)
@@ -71,7 +72,7 @@ def eigensolve_kpoints(inputs: list[dict], nbands: int, workers: int = 8, precis
                     hpsi = torch.zeros_like(psi)
                     t_k = time.perf_counter() - t0
                     r = E.eigensolve(ctx, psi, hpsi, nbands, d["mtxds"], d["hamsm"], d["hdiag"], epspsi=epspsi,
-                                     icmax=icmax, stream=stream.cuda_stream, trace=trace)
+                                     icmax=icmax, stream=stream.cuda_stream, trace=trace, ipr=ipr)
                 stream.synchronize()
                 if trace:
                     r["trace"][:, 0] += t_k          # times from the start of the set
