@@ -33,6 +33,7 @@ SIGNATURES = {
     "cpw_b200_wait_selftest": (I, [P, LL, P]),
     "cpw_b200_set_projector_slices": (I, [P, I]),
     "cpw_b200_zgemm_i8": (I, [P, I, I, I, I, P, LL, P, LL, C.c_double, I, P, LL, I, P]),
+    "cpw_b200_zgemm_i8_tri": (I, [P, I, I, I, I, P, LL, P, LL, C.c_double, I, P, LL, I, I, P]),
     "cpw_b200_timing_begin": (I, [P]),
     "cpw_b200_timing_end": (I, [P, DP, C.POINTER(C.c_longlong), I]),
     "cpw_b200_set_kpoint": (I, [P, I, IP, IP, I, DP, IP]),

@@ -464,7 +464,14 @@ int cpw_b200_set_projector_slices(cpw_b200_ctx* c, int slices) {
 
 int cpw_b200_zgemm_i8(cpw_b200_ctx* c, int transa, int m, int n, int k, const void* a, long long lda, const void* b,
                       long long ldb, double alpha, int accumulate, void* cm, long long ldc, int slices, void* stream) {
+  return cpw_b200_zgemm_i8_tri(c, transa, m, n, k, a, lda, b, ldb, alpha, accumulate, cm, ldc, slices, 0, stream);
+}
+
+int cpw_b200_zgemm_i8_tri(cpw_b200_ctx* c, int transa, int m, int n, int k, const void* a, long long lda,
+                          const void* b, long long ldb, double alpha, int accumulate, void* cm, long long ldc,
+                          int slices, int tri, void* stream) {
   if (int s = check_ctx(c)) return s;
+  if (tri < 0 || tri > 2) return fail(kBadArg, "zgemm_i8: tri must be 0, 1 or 2");
   if (transa != 'N' && transa != 'C') return fail(kBadArg, "zgemm_i8: transa must be 'N' or 'C'");
   if (m < 0 || n < 0 || k < 0) return fail(kBadArg, "zgemm_i8: negative dimension");
   const bool conj = transa == 'C';
@@ -472,7 +479,7 @@ int cpw_b200_zgemm_i8(cpw_b200_ctx* c, int transa, int m, int n, int k, const vo
     return fail(kBadArg, "zgemm_i8: leading dimension too small");
   cudaSetDevice(c->device);
   return oz_zgemm(c->ozs, conj, m, n, k, a, lda, b, ldb, alpha, accumulate != 0, cm, ldc, slices, c->tcs.wait_ns,
-                  stream ? (cudaStream_t)stream : c->stream);
+                  stream ? (cudaStream_t)stream : c->stream, tri);
 }
 
 int cpw_b200_timing_begin(cpw_b200_ctx* c) {

@@ -88,13 +88,20 @@ struct OzScratch {
   bool err_init = false;
 };
 int oz_prepare_a(OzOperand& op, bool conjA, int M, int K, const void* A, long long lda, int slices, cudaStream_t st);
+// triangular structure an int8 product may exploit (oz.cu)
+enum OzTri : int {
+  kOzFull = 0,
+  kOzLowerOut = 1,   // only the lower triangle of C (M = N) is wanted: tiles strictly above the diagonal are written as zeros
+  kOzUpperB = 2,     // B (K = N) is upper triangular: column block j reads only the first K rows it can reach
+};
 int oz_gemm_prepared(OzScratch& w, const OzOperand& op, int N, const void* B, long long ldb, double alpha,
-                     bool accumulate, void* C, long long ldc, unsigned long long wait_ns, cudaStream_t st);
+                     bool accumulate, void* C, long long ldc, unsigned long long wait_ns, cudaStream_t st,
+                     int tri = kOzFull);
 // C = alpha op(A) B (+ C) with op(A) = A or A^H, complex128 column-major, FP64-accurate on the
 // int8 tensor cores with `slices` 7-bit slices per operand (oz.cu)
 int oz_zgemm(OzScratch& w, bool conjA, int M, int N, int K, const void* A, long long lda, const void* B, long long ldb,
              double alpha, bool accumulate, void* C, long long ldc, int slices, unsigned long long wait_ns,
-             cudaStream_t st);
+             cudaStream_t st, int tri = kOzFull);
 int oz_read_error(OzScratch& w);
 int tc_error_flag(TcScratch& t);
 int tc_read_error(TcScratch& t);

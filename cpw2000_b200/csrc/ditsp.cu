@@ -375,15 +375,31 @@ struct Solver {
   // launches cost more than they save there)
   bool basis_i8 = false;
   int oz_slices = 7;
+  // which classes of basis-wide products take the int8 path when basis_i8 (CPW_B200_I8_PRODUCTS):
+  // the class of a product is read from the prefix of its name
+  enum : unsigned { kI8Chol = 1, kI8Mm = 2, kI8Conv = 4, kI8Span = 8, kI8Ham = 16, kI8Rot = 32, kI8Other = 64 };
+  // default: the Cholesky QR, the Ritz subspace Hamiltonian and the Ritz rotations (large square or
+  // tall products); the Gram-Schmidt passes against the converged block (many smaller products,
+  // each paying the operand splits) measured faster in cuBLAS FP64
+  unsigned i8_mask = kI8Chol | kI8Ham | kI8Rot;
+  static unsigned i8_class(const char* w) {
+    if (!strncmp(w, "cholqr", 6)) return kI8Chol;
+    if (!strncmp(w, "grsch_mm", 8)) return kI8Mm;
+    if (!strncmp(w, "grsch_loop", 10)) return kI8Conv;
+    if (!strncmp(w, "span", 4)) return kI8Span;
+    if (!strncmp(w, "ritz hamsm", 10)) return kI8Ham;
+    if (!strncmp(w, "ritz", 4)) return kI8Rot;
+    return kI8Other;
+  }
 
   long long n_i8 = 0, n_cublas = 0;
-  static constexpr double kI8MinFlops = 2e9;
+  double kI8MinFlops = 2e9;    // CPW_B200_I8_MIN_GFLOP
 
   // C(m x n) = alpha * op(A) * op(B) + beta * C
   int gemm(cublasOperation_t ta, cublasOperation_t tb, int mm, int nn, int kk, Z alpha, const Z* A, long long lda,
            const Z* Bm, long long ldb, Z beta, Z* Cm, long long ldc, const char* w) {
     if (mm <= 0 || nn <= 0) return kOk;
-    if (basis_i8 && kk > 0 && tb == CUBLAS_OP_N && (ta == CUBLAS_OP_N || ta == CUBLAS_OP_C) && alpha.y == 0 &&
+    if (basis_i8 && (i8_mask & i8_class(w)) && kk > 0 && tb == CUBLAS_OP_N && (ta == CUBLAS_OP_N || ta == CUBLAS_OP_C) && alpha.y == 0 &&
         (alpha.x == 1.0 || alpha.x == -1.0) && beta.y == 0 && (beta.x == 0.0 || beta.x == 1.0) &&
         8.0 * mm * nn * kk >= kI8MinFlops) {
       ++n_i8;
@@ -400,6 +416,19 @@ struct Solver {
       return kOk;
     }
     return ckb(cublasZgemm(blas, ta, tb, mm, nn, kk, &alpha, A, (int)lda, Bm, (int)ldb, &beta, Cm, (int)ldc), w);
+  }
+
+  // a product of the Cholesky QR: on the int8 tensor cores with its triangular structure (OzTri),
+  // else as gemm() routes it
+  bool oz_tri = true;
+  int chol_gemm(cublasOperation_t ta, int mm, int nn, int kk, const Z* A, long long lda, const Z* Bm, long long ldb,
+                Z* Cm, long long ldc, int tri, const char* w) {
+    if (basis_i8 && (i8_mask & kI8Chol) && 8.0 * mm * nn * kk >= kI8MinFlops) {
+      ++n_i8;
+      return oz_zgemm(c->ozs, ta == CUBLAS_OP_C, mm, nn, kk, A, lda, Bm, ldb, 1.0, false, Cm, ldc, oz_slices,
+                      c->tcs.wait_ns, st, oz_tri ? tri : kOzFull);
+    }
+    return gemm(ta, CUBLAS_OP_N, mm, nn, kk, one, A, lda, Bm, ldb, zero, Cm, ldc, w);
   }
 
   // host copies of per-column dots  out[j] = <x_j|y_j>
@@ -524,13 +553,12 @@ struct Solver {
   int apply_right_lh(Z* x, int k, const Z* Li) {
     if (int s = chol_tmp.ensure(sizeof(Z) * (size_t)m * k)) return s;
     Z* t = (Z*)chol_tmp.p;
-    if (basis_i8) {
+    if (basis_i8 && (i8_mask & kI8Chol)) {
       // the int8 GEMM takes B as stored: form Li^H
       if (int s = chol_lh.ensure(sizeof(Z) * (size_t)k * k)) return s;
       k_conj_transpose<<<std::max(1, std::min(1184, (int)(((long long)k * k + 255) / 256))), 256, 0, st>>>(
           Li, k, (Z*)chol_lh.p);
-      if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_N, m, k, k, one, x, m, (const Z*)chol_lh.p, k, zero, t, m,
-                       "cholqr apply"))
+      if (int s = chol_gemm(CUBLAS_OP_N, m, k, k, x, m, (const Z*)chol_lh.p, k, t, m, kOzUpperB, "cholqr apply"))
         return s;
     } else if (int s = gemm(CUBLAS_OP_N, CUBLAS_OP_C, m, k, k, one, x, m, Li, k, zero, t, m, "cholqr apply")) {
       return s;
@@ -576,8 +604,8 @@ struct Solver {
         if (chol_gram_gemm) {
           // X^H X as a full product: cuBLAS's zherk for a block of a few hundred vectors over
           // ~1e5 rows runs at a fraction of the ZGEMM rate (measured: 6 ms against ~1 ms)
-          if ((s = gemm(CUBLAS_OP_C, CUBLAS_OP_N, k, k, m, one, x, m, x, m, zero, G, k, "cholqr gram")))
-            return s;
+          // (the factorisation reads the lower triangle only)
+          if ((s = chol_gemm(CUBLAS_OP_C, k, k, m, x, m, x, m, G, k, kOzLowerOut, "cholqr gram"))) return s;
         } else {
           const double a1 = 1.0, b0 = 0.0;   // lower triangle of X^H X
           if (cublasZherk(blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, k, m, &a1, x, m, &b0, G, k) !=
@@ -802,7 +830,7 @@ struct Solver {
       const Z* xc = x + (size_t)c0 * m;
       // on the int8 tensor cores the converged block is split once for both passes: as A^H for
       // T = X^H Y, as A for Y -= X T (and H X for H Y -= H X T)
-      const bool i8 = basis_i8 && 8.0 * (nconv - c0) * k * m >= kI8MinFlops;
+      const bool i8 = basis_i8 && (i8_mask & kI8Conv) && 8.0 * (nconv - c0) * k * m >= kI8MinFlops;
       // (the splits live in the context: freeing device memory per call would synchronise the device)
       OzOperand& x_cn = c->oz_gs[0];
       OzOperand& x_nn = c->oz_gs[1];
@@ -1000,13 +1028,28 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
     if (!strcmp(v, "i8")) S.basis_i8 = true;
   }
   if (const char* v = getenv("CPW_B200_OZ_SLICES")) S.oz_slices = std::max(1, std::min(8, atoi(v)));
-  S.ham_full_gemm = S.basis_i8;
+  if (const char* v = getenv("CPW_B200_I8_PRODUCTS")) {
+    // comma list of chol, mm, conv, span, ham, rot, other, or all
+    const std::string l = std::string(",") + v + ",";
+    auto has = [&](const char* n) { return l.find(std::string(",") + n + ",") != std::string::npos; };
+    if (has("all")) {
+      S.i8_mask = ~0u;
+    } else {
+      S.i8_mask = (has("chol") ? Solver::kI8Chol : 0u) | (has("mm") ? Solver::kI8Mm : 0u) |
+                  (has("conv") ? Solver::kI8Conv : 0u) | (has("span") ? Solver::kI8Span : 0u) |
+                  (has("ham") ? Solver::kI8Ham : 0u) | (has("rot") ? Solver::kI8Rot : 0u) |
+                  (has("other") ? Solver::kI8Other : 0u);
+    }
+  }
+  S.ham_full_gemm = S.basis_i8 && (S.i8_mask & Solver::kI8Ham);
   if (const char* v = getenv("CPW_B200_HAM_BLOCK")) {
     if (!strcmp(v, "herkx")) S.ham_full_gemm = false;
     if (!strcmp(v, "gemm")) S.ham_full_gemm = true;
   }
   S.chol_gram_gemm = !(getenv("CPW_B200_CHOL_GRAM") && !strcmp(getenv("CPW_B200_CHOL_GRAM"), "herk"));
   S.chol_apply_gemm = !(getenv("CPW_B200_CHOL_APPLY") && !strcmp(getenv("CPW_B200_CHOL_APPLY"), "trsm"));
+  S.oz_tri = !(getenv("CPW_B200_OZ_TRI") && !strcmp(getenv("CPW_B200_OZ_TRI"), "0"));
+  if (const char* v = getenv("CPW_B200_I8_MIN_GFLOP")) S.kI8MinFlops = std::max(0.0, atof(v)) * 1e9;
   if (const char* o = getenv("CPW_B200_ORTHO")) {
     if (!strcmp(o, "mgs")) S.chol = false;
     if (!strcmp(o, "cholqr")) S.chol = true;
@@ -1511,7 +1554,7 @@ int ditsp_device(cpw_b200_ctx* c, int ipr, int* ifail, int icmax, int iguess, do
     // to the first zrows rows only
     const int cz = std::min(S.zcols, nsize);
     const Z* V = (const Z*)S.smallV.p;
-    if (S.tc_rot && !S.basis_i8) {
+    if (S.tc_rot && !(S.basis_i8 && (S.i8_mask & Solver::kI8Rot))) {
       if ((s = tc_zgemm_nn(c, mtxd, niter, nsize - cz, S.B(cz), mtxd, V + cz, nsize, PP, mtxd, st)) ||
           (cz > 0 && (s = tc_zgemm_nn(c, S.zrows, niter, cz, S.bas.p, mtxd, V, nsize, PP, mtxd, st, true))) ||
           (s = tc_zgemm_nn(c, mtxd, niter, nsize, S.hbas.p, mtxd, S.smallV.p, nsize, HPP, mtxd, st)))

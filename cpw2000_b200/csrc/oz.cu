@@ -62,6 +62,7 @@ constexpr int kBStages = 2;
 constexpr int kATile = BM * KBYTES;     // 16 KB
 constexpr int kBTile = BN * KBYTES;     // 8 KB
 constexpr int kMaxKbPerItem = 448;      // K blocks per int32 accumulation: 8 pairs x 57,344 x 64^2 < 2^31
+constexpr int kShortKb = 48;            // K blocks per work item by default (latency of one CTA)
 constexpr int kDrainWarps = 8;          // 4 lane quarters x 2 column halves
 constexpr int kThreads = 32 * (2 + kDrainWarps);
 constexpr int kTmemCols = 512;
@@ -84,6 +85,7 @@ struct Args {
   int tiles_m, tiles_n;        // tiles of 128 rows / 64 real columns
   double alpha;
   int accumulate;              // C += (nsplit == 1)
+  int tri;                     // OzTri: triangular structure of the product
   double2* c;
   long long ldc;
   double2* part;               // nsplit > 1: partials [split][N][M]
@@ -197,7 +199,15 @@ __device__ __forceinline__ Item item_of(const Args& g, int it) {
   w.m0 = w.mt * BM;
   w.n0 = w.nt * BN;
   w.kb0 = w.split * g.kb_per_split;
-  w.nblk = max(0, min(g.nkb, w.kb0 + g.kb_per_split) - w.kb0);
+  int klim = g.nkb;
+  if (g.tri == kOzUpperB) {
+    // complex columns [32 nt, 32 nt + 32) of an upper-triangular B have no nonzero below row
+    // 32 nt + 31: K blocks (64 complex rows each) from (nt + 2) / 2 on contribute nothing
+    klim = min(klim, (w.nt + 2) >> 1);
+  } else if (g.tri == kOzLowerOut && 32 * w.nt > w.mt * BM + BM - 1) {
+    klim = 0;                      // the tile lies strictly above the diagonal: written as zeros
+  }
+  w.nblk = max(0, min(klim, w.kb0 + g.kb_per_split) - w.kb0);
   w.rows_a = min(BM, g.M - w.m0);
   w.rows_b = min(BN, 2 * g.N - w.n0);
   return w;
@@ -677,11 +687,14 @@ int oz_prepare_a(OzOperand& op, bool conjA, int M, int K, const void* A, long lo
 
 // C = alpha op(A) B (+ C) with op(A) prepared by oz_prepare_a
 int oz_gemm_prepared(OzScratch& w, const OzOperand& op, int N, const void* B, long long ldb, double alpha,
-                     bool accumulate, void* C, long long ldc, unsigned long long wait_ns, cudaStream_t st) {
+                     bool accumulate, void* C, long long ldc, unsigned long long wait_ns, cudaStream_t st, int tri) {
   using namespace oz;
   const int M = op.M, K = op.K, s = op.s;
   if (M <= 0 || N <= 0) return kOk;
   if (!op.ready) return fail(kNotReady, "oz_zgemm: operand not prepared");
+  if (tri != kOzFull && tri != kOzLowerOut && tri != kOzUpperB) return fail(kBadArg, "oz_zgemm: unknown triangular mode");
+  if ((tri == kOzLowerOut && M != N) || (tri == kOzUpperB && K != N))
+    return fail(kBadArg, "oz_zgemm: triangular mode needs a square operand");
   cudaError_t e;
   if (K <= 0) {
     if (!accumulate) {
@@ -698,7 +711,15 @@ int oz_gemm_prepared(OzScratch& w, const OzOperand& op, int N, const void* B, lo
   // K splits: every split at most kMaxKbPerItem K blocks; among those, the count whose waves of
   // work items over the SMs finish first (waves x K blocks per item), fewer splits on ties
   const int tiles = tiles_m * tiles_n;
-  const int nmin = std::max(1, (nkb + kMaxKbPerItem - 1) / kMaxKbPerItem);
+  // K blocks per work item at most: the exactness bound, and a latency bound (CPW_B200_OZ_MAX_KB,
+  // default kShortKb) that keeps every CTA short, so that other streams' kernels (several
+  // k-points in flight) find free SMs within ~0.2 ms instead of waiting behind long items
+  const int max_kb = [] {
+    const char* v = getenv("CPW_B200_OZ_MAX_KB");
+    const int x = v ? atoi(v) : kShortKb;
+    return std::max(1, std::min(kMaxKbPerItem, x > 0 ? x : kMaxKbPerItem));
+  }();
+  const int nmin = std::max(1, (nkb + max_kb - 1) / max_kb);
   int nsplit = nmin;
   long long best = -1;
   for (int ns = nmin; ns <= std::min(nkb, nmin + 96); ++ns) {
@@ -746,6 +767,7 @@ int oz_gemm_prepared(OzScratch& w, const OzOperand& op, int N, const void* B, lo
   g.tiles_n = tiles_n;
   g.alpha = alpha;
   g.accumulate = accumulate ? 1 : 0;
+  g.tri = tri;
   g.c = (double2*)C;
   g.ldc = ldc;
   g.part = (double2*)w.part.p;
@@ -770,10 +792,10 @@ int oz_gemm_prepared(OzScratch& w, const OzOperand& op, int N, const void* B, lo
 // C = alpha op(A) B (+ C), complex128 column-major (see the head of this file)
 int oz_zgemm(OzScratch& w, bool conjA, int M, int N, int K, const void* A, long long lda, const void* B, long long ldb,
              double alpha, bool accumulate, void* C, long long ldc, int slices, unsigned long long wait_ns,
-             cudaStream_t st) {
+             cudaStream_t st, int tri) {
   if (M <= 0 || N <= 0) return kOk;
   if (int s = oz_prepare_a(w.aop, conjA, M, K, A, lda, slices, st)) return s;
-  return oz_gemm_prepared(w, w.aop, N, B, ldb, alpha, accumulate, C, ldc, wait_ns, st);
+  return oz_gemm_prepared(w, w.aop, N, B, ldb, alpha, accumulate, C, ldc, wait_ns, st, tri);
 }
 
 int oz_read_error(OzScratch& w) {

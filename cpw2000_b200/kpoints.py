@@ -29,6 +29,7 @@ def eigensolve_kpoints(inputs: list[dict], nbands: int, workers: int = 8, precis
 
     Returns (results, seconds): results[k] = dict(ei, neig, ihkpsum, converged) in input order,
     seconds the wall time of the whole set (inputs already on the host, contexts created inside).
+    icmax: outer iterations at most, one count for every k-point or a sequence with one per input.
     mxdbnd: columns of psi/hpsi (default nbands; the reference's array dimension, which bounds
     the iterative block). trace: also the per-iteration trace of each k-point (eigensolve's), with
     times from the common start of the set. keep: the first ``keep`` columns of each k-point's
@@ -45,6 +46,9 @@ def eigensolve_kpoints(inputs: list[dict], nbands: int, workers: int = 8, precis
     errors: list = []
     nw = max(1, min(int(workers), len(inputs)))
     mxdbnd = int(mxdbnd or nbands)
+    icmaxes = [int(v) for v in icmax] if hasattr(icmax, "__len__") else [int(icmax)] * len(inputs)
+    if len(icmaxes) != len(inputs):
+        raise ValueError("icmax: one count per k-point expected")
     saved = {k: os.environ.get(k) for k in (env or {})}
     os.environ.update(env or {})
     ctxs = [Context(device, precision=precision) for _ in range(nw)]
@@ -72,7 +76,7 @@ def eigensolve_kpoints(inputs: list[dict], nbands: int, workers: int = 8, precis
                     hpsi = torch.zeros_like(psi)
                     t_k = time.perf_counter() - t0
                     r = E.eigensolve(ctx, psi, hpsi, nbands, d["mtxds"], d["hamsm"], d["hdiag"], epspsi=epspsi,
-                                     icmax=icmax, stream=stream.cuda_stream, trace=trace, ipr=ipr)
+                                     icmax=icmaxes[k], stream=stream.cuda_stream, trace=trace, ipr=ipr)
                 stream.synchronize()
                 if trace:
                     r["trace"][:, 0] += t_k          # times from the start of the set

@@ -110,6 +110,15 @@ int cpw_b200_zgemm_i8(cpw_b200_ctx* ctx, int transa, int m, int n, int k, const 
                       const void* b, long long ldb, double alpha, int accumulate, void* c, long long ldc, int slices,
                       void* stream);
 
+/* cpw_b200_zgemm_i8 with a triangular structure it may exploit: tri 0 none;
+ * 1 only the lower triangle of C is wanted (m = n; output tiles strictly above
+ * the diagonal are written as zeros, the others in full); 2 B is upper
+ * triangular (k = n; the products with its zero part are skipped, so entries
+ * of B below the diagonal are treated as zero). */
+int cpw_b200_zgemm_i8_tri(cpw_b200_ctx* ctx, int transa, int m, int n, int k, const void* a, long long lda,
+                          const void* b, long long ldb, double alpha, int accumulate, void* c, long long ldc, int slices,
+                          int tri, void* stream);
+
 /* Stage timers (CUDA events around each kernel of a stage, on the stream the
  * kernel runs on). timing_end synchronises and writes per-stage totals in ms
  * and launch counts for stages 0..nstage-1: 0 scatter+inverse xy, 1 inverse z +
