@@ -796,6 +796,29 @@ def run_tte(args, local):
     print(json.dumps({"mode": "tte", **out}), flush=True)
 
 
+def run_kset(args, local):
+    """The eigensolver on the first --eig-kpoints k-points of the Si216 workload, --eig-workers in
+    flight, --icmax outer iterations, in the --precision form, with --env KEY=VALUE switches set
+    while it runs (--ipr 2 prints every k-point's phase times): the set's wall time and H|psi>
+    products. Studies of the eigensolver's switches under several k-points in flight."""
+    import torch
+
+    from cpw2000_b200 import hk_psi as H
+    from cpw2000_b200 import kpoints
+    torch.cuda.set_device(local)
+    w = configs.si216_cubic()
+    nk = max(1, min(args.eig_kpoints, len(w.kpoints)))
+    inputs = [configs.kpoint_inputs(w, k, with_hamsm=True) for k in range(nk)]
+    env = dict(kv.split("=", 1) for kv in args.env)
+    prec = {"fp64": H.FP64, "mixed": H.MIXED, "mixed_tc": H.MIXED_TC}[args.precision]
+    res, sec = kpoints.eigensolve_kpoints(inputs, NB, workers=min(args.eig_workers, nk), precision=prec,
+                                          icmax=args.icmax, device=local, mxdbnd=3 * NB, slab_budget=2 << 30,
+                                          env=env, ipr=args.ipr)
+    print(json.dumps({"mode": "kset", "precision": args.precision, "kpoints": nk, "in_flight": args.eig_workers,
+                      "icmax": args.icmax, "env": env, "seconds": sec,
+                      "hpsi_band_products": [int(r["ihkpsum"]) for r in res]}), flush=True)
+
+
 def run_eig_profile(args, local):
     """One eigensolver run on the Si216 Gamma point in one precision form (--precision), --icmax
     outer iterations, for ncu launch lists of the eigensolver's kernels."""
@@ -846,7 +869,8 @@ def run_profile(args, local):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--mode", choices=["bench", "profile", "eig", "gemm", "eigprof", "tte"], default="bench")
+    ap.add_argument("--mode", choices=["bench", "profile", "eig", "gemm", "eigprof", "tte", "kset"], default="bench")
+    ap.add_argument("--env", action="append", default=[], help="kset mode: KEY=VALUE switch (repeatable)")
     ap.add_argument("--slices", type=int, default=7, help="gemm mode: int8 slices")
     ap.add_argument("--nshapes", type=int, default=6, help="gemm mode: how many of the shapes")
     ap.add_argument("--workload", choices=["si216", "si64", "zb64"], default="si216", help="eig mode workload")
@@ -885,6 +909,8 @@ def main():
             run_eig_profile(args, local)
         elif args.mode == "tte":
             run_tte(args, local)
+        elif args.mode == "kset":
+            run_kset(args, local)
         elif args.impl == "reference":
             run_reference(args, rank)
         else:

@@ -276,14 +276,22 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
 // shared memory of k_z_vloc_pipe: work columns, two staging buffers of kept planes, twiddles, V tile
-template <typename T> inline size_t smem_columns_pipe(const LocalPlan& p, int cb) {
-  return smem_columns_pipe_bytes(sizeof(C2<T>), p, cb);
+template <typename T> inline size_t smem_columns_pipe(const LocalPlan& p, int cb, int nstage = 2) {
+  return smem_columns_pipe_bytes(sizeof(C2<T>), p, cb, nstage);
 }
 
-template <typename T, int RZ1, int RZ2, int CB, int NT = kThreadsCols>
-__global__ void __launch_bounds__(NT, pass_min_blocks(NT))
+// NSTAGE: kept-plane staging buffers (2: band b+1 streams in during band b; 1: it streams in
+// during the second and third pass of band b, which frees shared memory for a third CTA per SM).
+// MINB: CTAs per SM asked of the register allocator (0: the pass-size default).
+// TWREG: each thread keeps the z-twiddles of its own line in registers; it needs RZ1 == RZ2 and
+// NT == CB * RZ1, so that every thread owns the same line index in all three passes.
+template <typename T, int RZ1, int RZ2, int CB, int NT = kThreadsCols, int NSTAGE = 2, int MINB = 0,
+          bool TWREG = false>
+__global__ void __launch_bounds__(NT, MINB ? MINB : pass_min_blocks(NT))
 k_z_vloc_pipe(LocalPlan p, int nbc, int bands_per_group, const T* __restrict__ vr, const C2<T>* __restrict__ twz,
               C2<T>* __restrict__ W) {
+  static_assert(NSTAGE == 1 || NSTAGE == 2, "one or two staging buffers");
+  static_assert(!TWREG || (RZ1 == RZ2 && RZ1 > 0 && CB > 0 && NT == CB * RZ1), "register twiddles need one line per thread");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int cb = CB ? CB : p.cb;
   const int r1 = RZ1 ? RZ1 : p.dz.r1, r2 = RZ2 ? RZ2 : p.dz.r2;
@@ -291,7 +299,7 @@ k_z_vloc_pipe(LocalPlan p, int nbc, int bands_per_group, const T* __restrict__ v
   const int nz = p.nz;
   C2<T>* Cs = reinterpret_cast<C2<T>*>(smem_raw);
   C2<T>* Ws = Cs + (size_t)n3 * cb;
-  C2<T>* sz = Ws + 2 * (size_t)nz * cb;
+  C2<T>* sz = Ws + NSTAGE * (size_t)nz * cb;
   T* Vs = reinterpret_cast<T*>(sz + n3);
   const long long c0 = (long long)blockIdx.x * cb;
   const int ncol = (int)min((long long)cb, p.plane - c0);
@@ -315,13 +323,28 @@ k_z_vloc_pipe(LocalPlan p, int nbc, int bands_per_group, const T* __restrict__ v
   }
   stage(b_lo, 0);
   cp_async_commit();
-  if (b_lo + 1 < b_hi) stage(b_lo + 1, 1);
-  cp_async_commit();
+  if (NSTAGE == 2) {
+    if (b_lo + 1 < b_hi) stage(b_lo + 1, 1);
+    cp_async_commit();
+  }
+  // register twiddles: the thread's line index is tid / CB in every pass (n2i of pass 1, k1 of
+  // pass 2); W^(j a) for a = 1 .. R-1 (read once the twiddle table has been written)
+  C2<T> twr[TWREG ? RZ1 : 1];
+  bool tw_loaded = !TWREG;
 
   for (int b = b_lo; b < b_hi; ++b) {
-    const int buf = (b - b_lo) & 1;
-    cp_async_wait<1>();       // every group but the newest (band b+1) has landed
+    const int buf = NSTAGE == 2 ? (b - b_lo) & 1 : 0;
+    if (NSTAGE == 2)
+      cp_async_wait<1>();     // every group but the newest (band b+1) has landed
+    else
+      cp_async_wait<0>();     // band b has landed
     __syncthreads();
+    if (TWREG && !tw_loaded) {
+      const int j = tid / (CB ? CB : 1);
+#pragma unroll
+      for (int a = 0; a < (TWREG ? RZ1 : 1); ++a) twr[a] = sz[(j * a) % n3];
+      tw_loaded = true;
+    }
     const C2<T>* Wsb = Ws + (size_t)buf * nz * cb;
     // inverse pass 1 straight from the staged kept planes
     for (int it = tid; it < cb * r2; it += nt) {
@@ -337,14 +360,18 @@ k_z_vloc_pipe(LocalPlan p, int nbc, int bands_per_group, const T* __restrict__ v
           }
           DFT<RR, +1, T>::run(v);
 #pragma unroll
-          for (int a = 0; a < RR; ++a)
-            Cs[(size_t)(r2 * a + n2i) * cb + cl] = a == 0 ? v[0] : cmulc<T>(v[a], sz[n2i * a]);
+          for (int a = 0; a < RR; ++a) {
+            if constexpr (TWREG)
+              Cs[(size_t)(r2 * a + n2i) * cb + cl] = a == 0 ? v[0] : cmulc<T>(v[a], twr[a]);
+            else
+              Cs[(size_t)(r2 * a + n2i) * cb + cl] = a == 0 ? v[0] : cmulc<T>(v[a], sz[n2i * a]);
+          }
         });
       }
     }
     __syncthreads();
-    // the staging buffer of band b is free: prefetch band b+2 into it
-    if (b + 2 < b_hi) stage(b + 2, buf);
+    // the staging buffer of band b is free: prefetch band b+2 (two buffers) or b+1 (one) into it
+    if (b + NSTAGE < b_hi) stage(b + NSTAGE, buf);
     cp_async_commit();
     // inverse pass 2 -> V/N -> forward pass 1, in registers
     for (int it = tid; it < cb * r1; it += nt) {
@@ -360,8 +387,12 @@ k_z_vloc_pipe(LocalPlan p, int nbc, int bands_per_group, const T* __restrict__ v
           for (int a = 0; a < RR; ++a) v[a] = scal<T>(v[a], Vs[(size_t)(k1 + r1 * a) * cb + cl]);
           DFT<RR, -1, T>::run(v);
 #pragma unroll
-          for (int a = 0; a < RR; ++a)
-            Cs[(size_t)(r2 * k1 + a) * cb + cl] = a == 0 ? v[0] : cmul<T>(v[a], sz[k1 * a]);
+          for (int a = 0; a < RR; ++a) {
+            if constexpr (TWREG)
+              Cs[(size_t)(r2 * k1 + a) * cb + cl] = a == 0 ? v[0] : cmul<T>(v[a], twr[a]);
+            else
+              Cs[(size_t)(r2 * k1 + a) * cb + cl] = a == 0 ? v[0] : cmul<T>(v[a], sz[k1 * a]);
+          }
         });
       }
     }
@@ -563,7 +594,14 @@ cudaError_t launch_impl(const LocalPlan& p, int nbc, int band0, const C2<double>
   if (ev) cudaEventRecord(ev[0], st);
   ka<<<gA, NTP, sm_pl, st>>>(p, band0, psi, ldpsi, plane_start, pw_idx, pw_pos, twx, twy, W);
   if (ev) cudaEventRecord(ev[1], st);
-  const size_t sm_pipe = smem_columns_pipe<T>(p, p.cb);
+  // kernel B form on boxes whose z split is square (one line per thread in every pass):
+  // CPW_B200_ZB_VARIANT 1 = one staging buffer + 3 CTAs per SM, 2 = register twiddles,
+  // 3 = both; 0 = two staging buffers, twiddles in shared memory
+  int zv = 0;
+  if constexpr (RZ1 == RZ2 && RZ1 > 0 && CB > 0 && NTZ == CB * RZ1) {
+    if (const char* v = getenv("CPW_B200_ZB_VARIANT")) zv = std::max(0, std::min(3, atoi(v)));
+  }
+  const size_t sm_pipe = smem_columns_pipe<T>(p, p.cb, zv & 1 ? 1 : 2);
   const long long tiles = (p.plane + p.cb - 1) / p.cb;
   if (sm_pipe > (size_t)smax) {
     // the staged form does not fit: one CTA per (band, column tile)
@@ -578,6 +616,11 @@ cudaError_t launch_impl(const LocalPlan& p, int nbc, int band0, const C2<double>
     const int per = (int)((nbc + groups - 1) / groups);
     groups = (nbc + per - 1) / per;
     auto* kbp = k_z_vloc_pipe<T, RZ1, RZ2, CB, NTZ>;
+    if constexpr (RZ1 == RZ2 && RZ1 > 0 && CB > 0 && NTZ == CB * RZ1) {
+      if (zv == 1) kbp = k_z_vloc_pipe<T, RZ1, RZ2, CB, NTZ, 1, 3, false>;
+      if (zv == 2) kbp = k_z_vloc_pipe<T, RZ1, RZ2, CB, NTZ, 2, 0, true>;
+      if (zv == 3) kbp = k_z_vloc_pipe<T, RZ1, RZ2, CB, NTZ, 1, 3, true>;
+    }
     if ((e = smem_limit((const void*)kbp, (size_t)sm_pipe)) != cudaSuccess)
       return e;
     kbp<<<dim3((unsigned)tiles, (unsigned)groups), NTZ, sm_pipe, st>>>(p, nbc, per, vr, twz, W);

@@ -95,8 +95,8 @@ template <typename T> inline size_t smem_columns(const LocalPlan& p) {
 }
 // Staged (pipelined) form of kernel B: a column tile, two kept-plane buffers, the z-twiddles
 // and the potential columns; esz is the size of one complex element.
-inline size_t smem_columns_pipe_bytes(size_t esz, const LocalPlan& p, int cb) {
-  return esz * ((size_t)p.n3 * cb + 2 * (size_t)p.nz * cb + p.n3) + esz / 2 * (size_t)p.n3 * cb;
+inline size_t smem_columns_pipe_bytes(size_t esz, const LocalPlan& p, int cb, int nstage = 2) {
+  return esz * ((size_t)p.n3 * cb + (size_t)nstage * p.nz * cb + p.n3) + esz / 2 * (size_t)p.n3 * cb;
 }
 // Column tile of kernel B: 32 columns on short columns, 16 on columns of 128 points or more
 // and wherever the staged form would leave room for only one CTA per SM. Measured on a
