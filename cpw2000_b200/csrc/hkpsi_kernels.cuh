@@ -595,10 +595,13 @@ cudaError_t launch_impl(const LocalPlan& p, int nbc, int band0, const C2<double>
   ka<<<gA, NTP, sm_pl, st>>>(p, band0, psi, ldpsi, plane_start, pw_idx, pw_pos, twx, twy, W);
   if (ev) cudaEventRecord(ev[1], st);
   // kernel B form on boxes whose z split is square (one line per thread in every pass):
-  // CPW_B200_ZB_VARIANT 1 = one staging buffer + 3 CTAs per SM, 2 = register twiddles,
-  // 3 = both; 0 = two staging buffers, twiddles in shared memory
+  // CPW_B200_ZB_VARIANT 1 = one staging buffer + 3 CTAs per SM (the default there: on the 144^3
+  // box, 480 bands, FP64 B 8.58 -> 7.17 ms, FP32 5.38 -> 5.32 ms, identical results),
+  // 2 = register twiddles (FP32 6.49 ms), 3 = both; 0 = two staging buffers, twiddles in
+  // shared memory (the only form elsewhere)
   int zv = 0;
   if constexpr (RZ1 == RZ2 && RZ1 > 0 && CB > 0 && NTZ == CB * RZ1) {
+    zv = 1;
     if (const char* v = getenv("CPW_B200_ZB_VARIANT")) zv = std::max(0, std::min(3, atoi(v)));
   }
   const size_t sm_pipe = smem_columns_pipe<T>(p, p.cb, zv & 1 ? 1 : 2);

@@ -407,29 +407,37 @@ __global__ void __launch_bounds__(kThreads, 1) k_oz_gemm(const Args g) {
       asm volatile("tcgen05.fence::before_thread_sync;\n");
       __syncwarp();
       if (lane == 0) mbar_arrive(smem_u32(acce));
-      // rows of this lane, 16 complex columns of this half
+      // rows of this lane, 16 complex columns of this half, in two groups of 8 whose column
+      // exponents and (when accumulating) old C values are all loaded before the first store,
+      // so that their latencies overlap instead of adding up column by column
       const int i = w.m0 + 32 * quarter + lane;
       if (i < g.M) {
         const int ei = exp_or0(g.ea[i]);
         const int j0 = (w.n0 + 32 * half) >> 1;
+        const bool add_old = g.nsplit == 1 && g.accumulate;
 #pragma unroll
-        for (int c = 0; c < 16; ++c) {
-          const int j = j0 + c;
-          if (j < g.N) {
-            const double sc = ldexp(1.0, ei + exp_or0(g.eb[j]));
-            double re = acc[2 * c] * sc, im = acc[2 * c + 1] * sc;
-            if (g.nsplit > 1) {
-              g.part[((size_t)w.split * g.N + j) * g.M + i] = make_double2(re, im);
-            } else {
-              double2* cp = g.c + (size_t)j * g.ldc + i;
-              re *= g.alpha;
-              im *= g.alpha;
-              if (g.accumulate) {
-                const double2 o = *cp;
-                re += o.x;
-                im += o.y;
+        for (int c0 = 0; c0 < 16; c0 += 8) {
+          int ej[8];
+          double2 o[8];
+#pragma unroll
+          for (int c = 0; c < 8; ++c) {
+            const int j = j0 + c0 + c;
+            ej[c] = j < g.N ? exp_or0(g.eb[j]) : 0;
+            o[c] = add_old && j < g.N ? g.c[(size_t)j * g.ldc + i] : make_double2(0.0, 0.0);
+          }
+#pragma unroll
+          for (int c = 0; c < 8; ++c) {
+            const int j = j0 + c0 + c;
+            if (j < g.N) {
+              const double sc = ldexp(1.0, ei + ej[c]);
+              double re = acc[2 * (c0 + c)] * sc, im = acc[2 * (c0 + c) + 1] * sc;
+              if (g.nsplit > 1) {
+                g.part[((size_t)w.split * g.N + j) * g.M + i] = make_double2(re, im);
+              } else {
+                re = re * g.alpha + o[c].x;
+                im = im * g.alpha + o[c].y;
+                g.c[(size_t)j * g.ldc + i] = make_double2(re, im);
               }
-              *cp = make_double2(re, im);
             }
           }
         }
