@@ -285,8 +285,9 @@ template <typename T> inline size_t smem_columns_pipe(const LocalPlan& p, int cb
 // MINB: CTAs per SM asked of the register allocator (0: the pass-size default).
 // TWREG: each thread keeps the z-twiddles of its own line in registers; it needs RZ1 == RZ2 and
 // NT == CB * RZ1, so that every thread owns the same line index in all three passes.
+// VG: V(r)/N read from global memory (L2) in the middle pass instead of a shared-memory tile.
 template <typename T, int RZ1, int RZ2, int CB, int NT = kThreadsCols, int NSTAGE = 2, int MINB = 0,
-          bool TWREG = false>
+          bool TWREG = false, bool VG = false>
 __global__ void __launch_bounds__(NT, MINB ? MINB : pass_min_blocks(NT))
 k_z_vloc_pipe(LocalPlan p, int nbc, int bands_per_group, const T* __restrict__ vr, const C2<T>* __restrict__ twz,
               C2<T>* __restrict__ W) {
@@ -317,9 +318,11 @@ k_z_vloc_pipe(LocalPlan p, int nbc, int bands_per_group, const T* __restrict__ v
     }
   };
   for (int i = tid; i < n3; i += nt) sz[i] = twz[i];
-  for (int it = tid; it < cb * n3; it += nt) {
-    const int cl = it % cb, z = it / cb;
-    if (cl < ncol) cp_async_bytes(Vs + (size_t)z * cb + cl, vr + (size_t)z * p.plane + c0 + cl, (int)sizeof(T));
+  if (!VG) {
+    for (int it = tid; it < cb * n3; it += nt) {
+      const int cl = it % cb, z = it / cb;
+      if (cl < ncol) cp_async_bytes(Vs + (size_t)z * cb + cl, vr + (size_t)z * p.plane + c0 + cl, (int)sizeof(T));
+    }
   }
   stage(b_lo, 0);
   cp_async_commit();
@@ -380,11 +383,21 @@ k_z_vloc_pipe(LocalPlan p, int nbc, int bands_per_group, const T* __restrict__ v
         with_radix<RZ2>(r2, [&](auto rc_) {
           constexpr int RR = decltype(rc_)::value;
           C2<T> v[RR];
+          T vz[VG ? RR : 1];
+          if constexpr (VG) {
+#pragma unroll
+            for (int a = 0; a < RR; ++a) vz[a] = __ldg(vr + (size_t)(k1 + r1 * a) * p.plane + c0 + cl);
+          }
 #pragma unroll
           for (int a = 0; a < RR; ++a) v[a] = Cs[(size_t)(r2 * k1 + a) * cb + cl];
           DFT<RR, +1, T>::run(v);
 #pragma unroll
-          for (int a = 0; a < RR; ++a) v[a] = scal<T>(v[a], Vs[(size_t)(k1 + r1 * a) * cb + cl]);
+          for (int a = 0; a < RR; ++a) {
+            if constexpr (VG)
+              v[a] = scal<T>(v[a], vz[a]);
+            else
+              v[a] = scal<T>(v[a], Vs[(size_t)(k1 + r1 * a) * cb + cl]);
+          }
           DFT<RR, -1, T>::run(v);
 #pragma unroll
           for (int a = 0; a < RR; ++a) {
@@ -597,14 +610,16 @@ cudaError_t launch_impl(const LocalPlan& p, int nbc, int band0, const C2<double>
   // kernel B form on boxes whose z split is square (one line per thread in every pass):
   // CPW_B200_ZB_VARIANT 1 = one staging buffer + 3 CTAs per SM (the default there: on the 144^3
   // box, 480 bands, FP64 B 8.58 -> 7.17 ms, FP32 5.38 -> 5.32 ms, identical results),
-  // 2 = register twiddles (FP32 6.49 ms), 3 = both; 0 = two staging buffers, twiddles in
-  // shared memory (the only form elsewhere)
+  // 2 = register twiddles (FP32 6.49 ms), 3 = both, 4 = one staging buffer, V(r)/N from L2 and 4
+  // CTAs per SM, 5 = the same with 3 CTAs; 0 = two staging buffers, twiddles in shared memory (the
+  // only form elsewhere)
   int zv = 0;
   if constexpr (RZ1 == RZ2 && RZ1 > 0 && CB > 0 && NTZ == CB * RZ1) {
     zv = 1;
-    if (const char* v = getenv("CPW_B200_ZB_VARIANT")) zv = std::max(0, std::min(3, atoi(v)));
+    if (const char* v = getenv("CPW_B200_ZB_VARIANT")) zv = std::max(0, std::min(5, atoi(v)));
   }
-  const size_t sm_pipe = smem_columns_pipe<T>(p, p.cb, zv & 1 ? 1 : 2);
+  size_t sm_pipe = smem_columns_pipe<T>(p, p.cb, zv == 1 || zv >= 3 ? 1 : 2);
+  if (zv >= 4) sm_pipe -= sizeof(T) * (size_t)p.n3 * p.cb;     // no V tile
   const long long tiles = (p.plane + p.cb - 1) / p.cb;
   if (sm_pipe > (size_t)smax) {
     // the staged form does not fit: one CTA per (band, column tile)
@@ -623,6 +638,8 @@ cudaError_t launch_impl(const LocalPlan& p, int nbc, int band0, const C2<double>
       if (zv == 1) kbp = k_z_vloc_pipe<T, RZ1, RZ2, CB, NTZ, 1, 3, false>;
       if (zv == 2) kbp = k_z_vloc_pipe<T, RZ1, RZ2, CB, NTZ, 2, 0, true>;
       if (zv == 3) kbp = k_z_vloc_pipe<T, RZ1, RZ2, CB, NTZ, 1, 3, true>;
+      if (zv == 4) kbp = k_z_vloc_pipe<T, RZ1, RZ2, CB, NTZ, 1, 4, false, true>;
+      if (zv == 5) kbp = k_z_vloc_pipe<T, RZ1, RZ2, CB, NTZ, 1, 3, false, true>;
     }
     if ((e = smem_limit((const void*)kbp, (size_t)sm_pipe)) != cudaSuccess)
       return e;
