@@ -15,7 +15,8 @@ the reference-facing C ABI (cpw_b200_hk_psi_c16) on pinned host arrays, the H2D
 copy of psi and the D2H copy of hpsi inside the timed region. time_to_eigvals:
 the eigensolver (ditsp_c16 restated) on Gamma and the 3 random k-points of the
 workload, FP64 drop-in vs the mixed form, to 1e-6 Ha (both) and 1e-8 Ha (FP64),
-median of R repeats, then adjoint forces of both converged sets at Gamma.
+median of R repeats, then adjoint forces of both converged sets at Gamma (on by default on
+one GPU; --gpus N > 1 runs the H|psi> replicas only unless --eig 1 is given).
 --impl reference times the CPU restatement of the reference's hk_psi_c16
 (C + OpenMP, all host threads) on the same workload, a sample of bands per step.
 """
@@ -891,13 +892,16 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--eig", type=int, default=1, help="also measure time-to-eigvals (1) or not (0)")
+    ap.add_argument("--eig", type=int, default=None, help="also measure time-to-eigvals (1) or not (0); default 1 on "
+                    "one GPU, 0 on several (the replicas' H|psi> scaling run stays short)")
     ap.add_argument("--eig-repeats", type=int, default=3, help="repeats of the time-to-eigvals sets (median)")
     ap.add_argument("--eig-kpoints", type=int, default=4, help="k-points of the Si216 workload solved (Gamma first)")
     ap.add_argument("--eig-workers", type=int, default=4, help="k-points in flight during the eigensolver sets")
     ap.add_argument("--eig-budget", type=float, default=560.0, help="seconds the eigensolver repeats may take")
     args = ap.parse_args()
     world, rank, local, dist = dist_setup(args)
+    if args.eig is None:
+        args.eig = 1 if world == 1 else 0
     try:
         if args.mode == "profile":
             run_profile(args, local)
