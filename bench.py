@@ -729,7 +729,8 @@ def run_gemm(args, local):
     shapes = [("C", 1000, 180, 88951), ("N", 88951, 180, 1000), ("C", 180, 180, 88951), ("N", 88951, 490, 1160),
               ("C", 864, 480, 88951), ("N", 88951, 480, 864)]
     out = {"mode": "gemm", "slices": args.slices, "shapes": []}
-    for ta, m, n, k in shapes[: args.nshapes]:
+    chosen = [shapes[args.shape_index]] if args.shape_index >= 0 else shapes[: args.nshapes]
+    for ta, m, n, k in chosen:
         a = torch.randn((k, m) if ta == "C" else (m, k), dtype=torch.complex128, device=dev)
         a = a.t().contiguous().t()                   # column-major
         b = torch.randn((k, n), dtype=torch.complex128, device=dev).t().contiguous().t()
@@ -874,6 +875,7 @@ def main():
     ap.add_argument("--env", action="append", default=[], help="kset mode: KEY=VALUE switch (repeatable)")
     ap.add_argument("--slices", type=int, default=7, help="gemm mode: int8 slices")
     ap.add_argument("--nshapes", type=int, default=6, help="gemm mode: how many of the shapes")
+    ap.add_argument("--shape-index", type=int, default=-1, help="gemm mode: this one shape only (0-5)")
     ap.add_argument("--workload", choices=["si216", "si64", "zb64"], default="si216", help="eig mode workload")
     ap.add_argument("--icmax", type=int, default=200, help="eig mode: outer iterations at most")
     ap.add_argument("--epspsi", type=float, default=1e-5, help="eig mode: residual tolerance")

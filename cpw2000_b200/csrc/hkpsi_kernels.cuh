@@ -52,7 +52,7 @@ k_inv_xy(LocalPlan p, int band0, const C2<double>* __restrict__ psi, long long l
   C2<T>* sx = Tb + (size_t)n2 * tc;
   C2<T>* sy = sx + n1;
   const int zi = blockIdx.x, b = blockIdx.y;
-  const int tid = threadIdx.x, nt = blockDim.x;
+  const int tid = threadIdx.x, nt = NT;     // every launch uses NT threads
 
   const C2<double>* ps = psi + (size_t)(band0 + b) * ldpsi;
   if (p.kdesc) {      // batch of k-points: this band's own basis and block
@@ -307,7 +307,7 @@ k_z_vloc_pipe(LocalPlan p, int nbc, int bands_per_group, const T* __restrict__ v
   const int b_lo = blockIdx.y * bands_per_group;
   const int b_hi = min(nbc, b_lo + bands_per_group);
   if (b_lo >= b_hi) return;
-  const int tid = threadIdx.x, nt = blockDim.x;
+  const int tid = threadIdx.x, nt = NT;     // every launch uses NT threads
 
   auto stage = [&](int b, int buf) {
     const C2<T>* Wb = W + (size_t)b * nz * (size_t)p.plane + c0;
@@ -454,7 +454,7 @@ k_fwd_xy(LocalPlan p, int band0, const C2<double>* __restrict__ psi, long long l
   C2<T>* sx = Tb + (size_t)n2 * tc;
   C2<T>* sy = sx + n1;
   const int zi = blockIdx.x, b = blockIdx.y;
-  const int tid = threadIdx.x, nt = blockDim.x;
+  const int tid = threadIdx.x, nt = NT;     // every launch uses NT threads
   for (int i = tid; i < n1; i += nt) sx[i] = twx[i];
   for (int i = tid; i < n2; i += nt) sy[i] = twy[i];
   const C2<double>* ps = psi + (size_t)(band0 + b) * ldpsi;
