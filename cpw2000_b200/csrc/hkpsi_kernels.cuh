@@ -334,6 +334,15 @@ k_z_vloc_pipe(LocalPlan p, int nbc, int bands_per_group, const T* __restrict__ v
   // pass 2); W^(j a) for a = 1 .. R-1 (read once the twiddle table has been written)
   C2<T> twr[TWREG ? RZ1 : 1];
   bool tw_loaded = !TWREG;
+  // one pass-1 / pass-3 line per thread (line index j = tid / CB in both): the kept-plane index
+  // of each of its points z = RZ2 a + j, fixed for all bands, is computed once (FP32: the FP64
+  // form has no registers to spare for it under its 3-CTA bound)
+  constexpr bool kOneLine = sizeof(T) == 4 && CB > 0 && RZ1 > 0 && RZ2 > 0 && NT == CB * RZ2;
+  int zk[kOneLine ? RZ1 : 1];
+  if constexpr (kOneLine) {
+#pragma unroll
+    for (int a = 0; a < RZ1; ++a) zk[a] = idx_to_kept(RZ2 * a + tid / CB, p.kd3, n3, nz);
+  }
 
   for (int b = b_lo; b < b_hi; ++b) {
     const int buf = NSTAGE == 2 ? (b - b_lo) & 1 : 0;
@@ -358,7 +367,11 @@ k_z_vloc_pipe(LocalPlan p, int nbc, int bands_per_group, const T* __restrict__ v
           C2<T> v[RR];
 #pragma unroll
           for (int a = 0; a < RR; ++a) {
-            const int zi = idx_to_kept(r2 * a + n2i, p.kd3, n3, nz);
+            int zi;
+            if constexpr (kOneLine)
+              zi = zk[a];
+            else
+              zi = idx_to_kept(r2 * a + n2i, p.kd3, n3, nz);
             v[a] = zi >= 0 ? Wsb[(size_t)zi * cb + cl] : czero<T>();
           }
           DFT<RR, +1, T>::run(v);
@@ -423,7 +436,11 @@ k_z_vloc_pipe(LocalPlan p, int nbc, int bands_per_group, const T* __restrict__ v
           DFT<RR, -1, T>::run(v);
 #pragma unroll
           for (int a = 0; a < RR; ++a) {
-            const int zi = idx_to_kept(m2 + r2 * a, p.kd3, n3, nz);
+            int zi;
+            if constexpr (kOneLine)
+              zi = zk[a];
+            else
+              zi = idx_to_kept(m2 + r2 * a, p.kd3, n3, nz);
             if (zi >= 0) Wb[(size_t)zi * p.plane + cl] = v[a];
           }
         });
