@@ -133,7 +133,8 @@ def cpu_reference_rate(d, nbands: int, nthreads: int = 0, repeats: int = 1):
     return nbands / min(times), (nthreads or c_ref.max_threads())
 
 
-def time_to_eigvals(w, inputs, local, repeats=3, workers=4, icmax=300, nocc=None, budget_s=480.0):
+def time_to_eigvals(w, inputs, local, repeats=3, workers=4, icmax=300, nocc=None, budget_s=480.0,
+                    prioritise=False):
     """Eigensolver (ditsp_c16 restated) on the k-points of the Si216 workload, FP64 drop-in vs mixed.
 
     Each repeat solves every k-point of ``inputs`` (Gamma + 3 random k) from the start basis
@@ -161,6 +162,7 @@ def time_to_eigvals(w, inputs, local, repeats=3, workers=4, icmax=300, nocc=None
     runs = {name: [] for name, _ in forms}
     keep = {}
     icmax_rep = {name: icmax for name, _ in forms}
+    prio_rep = {name: None for name, _ in forms}
     t_start = time.perf_counter()
     refs = None
     for rep in range(repeats):
@@ -168,7 +170,8 @@ def time_to_eigvals(w, inputs, local, repeats=3, workers=4, icmax=300, nocc=None
         for name, prec in forms:
             res, secs = kpoints.eigensolve_kpoints(inputs, NB, workers=workers, precision=prec, epspsi=1e-5,
                                                    icmax=icmax_rep[name], device=local, mxdbnd=3 * NB, trace=True,
-                                                   keep=nocc if rep == 0 else 0, slab_budget=2 << 30)
+                                                   keep=nocc if rep == 0 else 0, slab_budget=2 << 30,
+                                                   priorities=prio_rep[name])
             if rep == 0:
                 keep[name] = res[0].pop("psi")
                 for r in res[1:]:
@@ -188,6 +191,13 @@ def time_to_eigvals(w, inputs, local, repeats=3, workers=4, icmax=300, nocc=None
                     ok = np.nonzero(err <= tol)[0]
                     per_k.append(min(icmax, (int(ok[0]) + 1 if len(ok) else r["trace"].shape[0]) + 5))
                 icmax_rep[name] = per_k
+                if prioritise:
+                    # longest solve first: stream priority by the first repeat's iteration counts
+                    rank = sorted(range(len(per_k)), key=lambda k: -per_k[k])
+                    prio = [0] * len(per_k)
+                    for r_, k in enumerate(rank):
+                        prio[k] = -(len(per_k) - 1 - r_)
+                    prio_rep[name] = prio
         dt = time.perf_counter() - t_rep
         if time.perf_counter() - t_start + 0.8 * dt > budget_s:
             break
@@ -207,7 +217,7 @@ def time_to_eigvals(w, inputs, local, repeats=3, workers=4, icmax=300, nocc=None
     out = {"kpoints": [[float(x) for x in w.kpoints[k]] for k in range(len(inputs))],
            "mtxd": [int(d["mtxd"]) for d in inputs], "occupied": nocc, "repeats": len(runs["fp64"]),
            "repeats_asked": repeats, "kpoints_in_flight": workers, "icmax_first": icmax,
-           "icmax_later": icmax_rep}
+           "icmax_later": icmax_rep, "stream_priorities_later": prio_rep}
     for name, _ in forms:
         tols = (1e-6, 1e-8) if name == "fp64" else (1e-6,)
         entry = {}
@@ -794,7 +804,7 @@ def run_tte(args, local):
     nk = max(1, min(args.eig_kpoints, len(w.kpoints)))
     inputs = [configs.kpoint_inputs(w, k, with_hamsm=True) for k in range(nk)]
     out = time_to_eigvals(w, inputs, local, repeats=args.eig_repeats, workers=min(args.eig_workers, nk),
-                          budget_s=args.eig_budget)
+                          budget_s=args.eig_budget, prioritise=bool(args.eig_priorities))
     print(json.dumps({"mode": "tte", **out}), flush=True)
 
 
@@ -900,6 +910,8 @@ def main():
     ap.add_argument("--eig-kpoints", type=int, default=4, help="k-points of the Si216 workload solved (Gamma first)")
     ap.add_argument("--eig-workers", type=int, default=4, help="k-points in flight during the eigensolver sets")
     ap.add_argument("--eig-budget", type=float, default=560.0, help="seconds the eigensolver repeats may take")
+    ap.add_argument("--eig-priorities", type=int, default=0, help="later eigensolver repeats: stream priority by the "
+                    "first repeat's per-k iteration counts (1) or equal priorities (0)")
     args = ap.parse_args()
     world, rank, local, dist = dist_setup(args)
     if args.eig is None:

@@ -24,7 +24,8 @@ from .hk_psi import FP64, Context
 
 def eigensolve_kpoints(inputs: list[dict], nbands: int, workers: int = 8, precision: int = FP64, epspsi=1e-5,
                        icmax=60, device: int = 0, seed: int = 0, mxdbnd: int | None = None, trace: bool = False,
-                       keep: int = 0, slab_budget: int = 0, env: dict | None = None, ipr: int = 0):
+                       keep: int = 0, slab_budget: int = 0, env: dict | None = None, ipr: int = 0,
+                       priorities: list[int] | None = None):
     """Run ditsp for every k-point dict of ``inputs`` (configs.kpoint_inputs(..., with_hamsm=True)).
 
     Returns (results, seconds): results[k] = dict(ei, neig, ihkpsum, converged) in input order,
@@ -36,11 +37,16 @@ def eigensolve_kpoints(inputs: list[dict], nbands: int, workers: int = 8, precis
     converged psi are returned (device tensors, ``psi``). slab_budget: FFT slab bytes per context.
     env: environment variables set while the set runs (the eigensolver reads its switches then).
     ipr: the eigensolver's print level (2: per-phase wall times of every k-point).
+    priorities: CUDA stream priority of each k-point's solve (lower = scheduled first, within the
+    device's range, e.g. -5 .. 0); k-points are also taken from the queue in that order. An SCF
+    code can rank k-points by the outer iterations their previous solve took, so that the longest
+    solve is not held back by the others (longest-processing-time-first).
     """
     import torch
     dev = torch.device("cuda", device)
     todo: queue.Queue = queue.Queue()
-    for k in range(len(inputs)):
+    order = sorted(range(len(inputs)), key=lambda k: priorities[k]) if priorities else range(len(inputs))
+    for k in order:
         todo.put(k)
     results: list = [None] * len(inputs)
     errors: list = []
@@ -62,13 +68,17 @@ def eigensolve_kpoints(inputs: list[dict], nbands: int, workers: int = 8, precis
     torch.cuda.synchronize(dev)
 
     def work(ctx: Context):
-        stream = torch.cuda.Stream(device=dev)
+        streams: dict = {}
         try:
             while True:
                 try:
                     k = todo.get_nowait()
                 except queue.Empty:
                     return
+                pr = int(priorities[k]) if priorities else 0
+                if pr not in streams:
+                    streams[pr] = torch.cuda.Stream(device=dev, priority=pr)
+                stream = streams[pr]
                 d = inputs[k]
                 ctx.setup(d)
                 with torch.cuda.stream(stream):
