@@ -57,6 +57,27 @@ int default_ctx(cpw_b200_ctx** out) {
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     int s = cpw_b200_create(&g_default, dev);
     if (s) return s;
+    // the drop-in entry points (hk_psi_c16_, hk_psi_nl_c16_, ditsp_c16_, ...) take no context: a
+    // host code that links them unchanged selects their form by environment, read once here
+    int mode = CPW_B200_FP64;
+    if (const char* v = getenv("CPW_B200_DROPIN_PRECISION")) {
+      if (!strcmp(v, "mixed")) {
+        mode = CPW_B200_MIXED;
+      } else if (!strcmp(v, "mixed_tc")) {
+        mode = CPW_B200_MIXED_TC;
+      } else if (strcmp(v, "fp64") != 0) {
+        cpw_b200_destroy(g_default);
+        g_default = nullptr;
+        return fail(kBadArg, "CPW_B200_DROPIN_PRECISION must be fp64, mixed or mixed_tc");
+      }
+    }
+    if (!s && mode != CPW_B200_FP64) s = cpw_b200_set_precision(g_default, mode);
+    if (const char* v = getenv("CPW_B200_DROPIN_PROJECTOR_SLICES"); !s && v) s = cpw_b200_set_projector_slices(g_default, atoi(v));
+    if (s) {
+      cpw_b200_destroy(g_default);
+      g_default = nullptr;
+      return s;
+    }
   }
   *out = g_default;
   return kOk;
