@@ -687,7 +687,7 @@ def run_ours(args, world, rank, local, dist):
 
 
 def si64_throughput(local, steps, warmup):
-    """H|psi> of the Si64 workload (configs[1]: 26,529 PW, 96^3, 256 projectors, 160 bands): FP64 and
+    """H|psi> of the Si64 workload (the 64-atom cubic cell: 26,529 PW, 96^3, 256 projectors, 160 bands): FP64 and
     MIXED_TC bands/s, device-resident, L2 flushed (256 MiB memset) before each timed step."""
     import torch
 
