@@ -133,6 +133,49 @@ def cpu_reference_rate(d, nbands: int, nthreads: int = 0, repeats: int = 1):
     return nbands / min(times), (nthreads or c_ref.max_threads())
 
 
+def first_within(trace, ref, nocc, tol):
+    """0-based outer iteration at which the lowest nocc Ritz values of an eigensolver trace (rows:
+    elapsed s, xmax, nconv, H|psi> products, eigenvalues...) are all within tol of ref, or None."""
+    err = np.abs(trace[:, 4:4 + nocc] - ref[None, :]).max(axis=1)
+    ok = np.nonzero(err <= tol)[0]
+    return int(ok[0]) if len(ok) else None
+
+
+def stop_iterations(results, refs, nocc, tol, icmax, margin=5):
+    """Per k-point outer-iteration limit of a later repeat: `margin` iterations past the one at which
+    the first repeat met the tolerance (all its iterations when it never did), at most icmax."""
+    per_k = []
+    for r, ref in zip(results, refs):
+        i = first_within(r["trace"], ref, nocc, tol)
+        per_k.append(min(icmax, (i + 1 if i is not None else r["trace"].shape[0]) + margin))
+    return per_k
+
+
+def longest_first_priorities(per_k):
+    """CUDA stream priorities (lower runs first) ranking k-points by their iteration counts: the
+    longest solve gets -(n-1), the shortest 0; ties keep input order."""
+    rank = sorted(range(len(per_k)), key=lambda k: -per_k[k])
+    prio = [0] * len(per_k)
+    for pos, k in enumerate(rank):
+        prio[k] = -(len(per_k) - 1 - pos)
+    return prio
+
+
+def set_time(results, refs, nocc, tol):
+    """(seconds, iterations per k-point, H|psi> band products) until every k-point met the tolerance:
+    the latest k-point's time (traces hold times from the start of the set), or (None, None, None)
+    if one never did."""
+    ts, its, hk = [], [], 0
+    for r, ref in zip(results, refs):
+        i = first_within(r["trace"], ref, nocc, tol)
+        if i is None:
+            return None, None, None
+        ts.append(float(r["trace"][i, 0]))
+        its.append(i + 1)
+        hk += int(r["trace"][i, 3])
+    return max(ts), its, hk
+
+
 def time_to_eigvals(w, inputs, local, repeats=3, workers=4, icmax=300, nocc=None, budget_s=480.0,
                     prioritise=False):
     """Eigensolver (ditsp_c16 restated) on the k-points of the Si216 workload, FP64 drop-in vs mixed.
@@ -185,34 +228,13 @@ def time_to_eigvals(w, inputs, local, repeats=3, workers=4, icmax=300, nocc=None
             # not keep running beside the others)
             for name, _ in forms:
                 tol = 1e-8 if name == "fp64" else 1e-6
-                per_k = []
-                for r, ref in zip(runs[name][0][0], refs):
-                    err = np.abs(r["trace"][:, 4:4 + nocc] - ref[None, :]).max(axis=1)
-                    ok = np.nonzero(err <= tol)[0]
-                    per_k.append(min(icmax, (int(ok[0]) + 1 if len(ok) else r["trace"].shape[0]) + 5))
-                icmax_rep[name] = per_k
+                icmax_rep[name] = stop_iterations(runs[name][0][0], refs, nocc, tol, icmax)
                 if prioritise:
                     # longest solve first: stream priority by the first repeat's iteration counts
-                    rank = sorted(range(len(per_k)), key=lambda k: -per_k[k])
-                    prio = [0] * len(per_k)
-                    for r_, k in enumerate(rank):
-                        prio[k] = -(len(per_k) - 1 - r_)
-                    prio_rep[name] = prio
+                    prio_rep[name] = longest_first_priorities(icmax_rep[name])
         dt = time.perf_counter() - t_rep
         if time.perf_counter() - t_start + 0.8 * dt > budget_s:
             break
-
-    def set_time(res, tol):
-        ts, its, hk = [], [], 0
-        for r, ref in zip(res, refs):
-            err = np.abs(r["trace"][:, 4:4 + nocc] - ref[None, :]).max(axis=1)
-            ok = np.nonzero(err <= tol)[0]
-            if not len(ok):
-                return None, None, None
-            ts.append(float(r["trace"][ok[0], 0]))
-            its.append(int(ok[0]) + 1)
-            hk += int(r["trace"][ok[0], 3])
-        return max(ts), its, hk
 
     out = {"kpoints": [[float(x) for x in w.kpoints[k]] for k in range(len(inputs))],
            "mtxd": [int(d["mtxd"]) for d in inputs], "occupied": nocc, "repeats": len(runs["fp64"]),
@@ -222,7 +244,7 @@ def time_to_eigvals(w, inputs, local, repeats=3, workers=4, icmax=300, nocc=None
         tols = (1e-6, 1e-8) if name == "fp64" else (1e-6,)
         entry = {}
         for tol in tols:
-            vals = [set_time(res, tol) for res, _ in runs[name]]
+            vals = [set_time(res, refs, nocc, tol) for res, _ in runs[name]]
             times = [v[0] for v in vals if v[0] is not None]
             key = f"{tol:.0e}".replace("e-0", "e-")
             entry[f"seconds_to_{key}_ha"] = statistics.median(times) if len(times) == len(vals) else None
