@@ -70,3 +70,62 @@ def test_roofline_of_counts_algorithmic_bytes():
     assert r["achieved"] == pytest.approx(alg / 1e-3 / 1e9)
     assert r["frac"] == pytest.approx(r["achieved"] / 6538.0)
     assert r["traffic"] == 12345 * 20
+
+
+def test_time_to_eigvals_bookkeeping_with_fake_solves(monkeypatch):
+    # the whole time-to-eigenvalues procedure on the CPU, with the eigensolver and the forces
+    # replaced by fakes: the error falls by 10 decades in 10 + 5k iterations for FP64 and in 6 + 3k
+    # for the mixed form, down to a 1e-7 floor; later repeats must receive the per-k stop counts
+    from types import SimpleNamespace
+
+    from cpw2000_b200 import forces as FF
+    from cpw2000_b200 import hk_psi as H
+    from cpw2000_b200 import kpoints
+
+    nocc = 2
+    exact = np.array([-1.0, 0.5])
+    calls = []
+
+    def fake_solve(inputs, nbands, workers, precision, icmax, keep=0, priorities=None, **kw):
+        calls.append((precision, icmax if np.isscalar(icmax) else list(icmax), priorities))
+        res = []
+        for k, _ in enumerate(inputs):
+            n = icmax if np.isscalar(icmax) else icmax[k]
+            slow = 10 + 5 * k if precision == H.FP64 else 6 + 3 * k
+            it = np.arange(n)
+            err = np.maximum(0.5 * 10.0 ** (-(it + 1) * 10.0 / slow), 0.0 if precision == H.FP64 else 1e-7)
+            tr = np.zeros((n, 4 + 8))
+            tr[:, 0] = 0.1 * (it + 1) * (2.0 if precision == H.FP64 else 1.0)
+            tr[:, 3] = 50 * (it + 1)
+            tr[:, 4:4 + nocc] = exact[None, :] + err[:, None]
+            r = {"trace": tr, "converged": False}
+            if keep:
+                r["psi"] = np.zeros((4, keep))
+            res.append(r)
+        return res, float(tr[-1, 0])
+
+    class FakeSystem:
+        def __init__(self, w, d, psi, occ, device=0):
+            self.ctx = SimpleNamespace(close=lambda: None)
+
+    monkeypatch.setattr(kpoints, "eigensolve_kpoints", fake_solve)
+    monkeypatch.setattr(FF, "HFSystem", FakeSystem)
+    monkeypatch.setattr(FF, "forces", lambda s: (0.0, np.zeros((1, 3))))
+    monkeypatch.setattr(FF, "to_cartesian", lambda f, adot: np.array([[0.1, 0.0, 0.0]]))
+    w = SimpleNamespace(species=[SimpleNamespace(natom=1)], kpoints=[(0, 0, 0), (0.1, 0, 0)], adot=np.eye(3))
+    inputs = [{"mtxd": 10}, {"mtxd": 11}]
+    out = bench.time_to_eigvals(w, inputs, 0, repeats=3, workers=2, icmax=40, nocc=nocc, budget_s=1e9,
+                                prioritise=True)
+    assert out["repeats"] == 3
+    # FP64 at 1e-8 within 8 iterations of k0 (slow 10) and 12 of k1 (slow 15): stop at 13 and 17
+    assert out["icmax_later"]["fp64"] == [8 + 5, 12 + 5]
+    assert out["stream_priorities_later"]["fp64"] == [0, -1]
+    assert calls[2] == (H.FP64, [13, 17], [0, -1])
+    # the mixed form reaches 1e-6 but not 1e-8 (floor 1e-7)
+    assert out["mixed_tc"]["iterations_to_1e-6_ha"] == [4, 6]
+    assert out["fp64"]["iterations_to_1e-6_ha"] == [6, 9]
+    # times: FP64 0.2 s per iteration, mixed 0.1 s; the set time is the slower k-point's
+    assert out["fp64"]["seconds_to_1e-6_ha"] == pytest.approx(1.8)
+    assert out["mixed_tc"]["seconds_to_1e-6_ha"] == pytest.approx(0.6)
+    assert out["speedup_mixed_tc_vs_fp64_at_1e-6"] == pytest.approx(3.0)
+    assert out["force_max_abs_diff_ha_bohr"] == 0.0
