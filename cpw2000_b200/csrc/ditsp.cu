@@ -122,8 +122,9 @@ __global__ void k_colscale(int m, Z* __restrict__ x, long long ldx, const double
 // with every decision taken on the device: sequential MGS projections, the
 // repeat when xnp > 0.9999 xni, the drop below 1e-20 of the natural scale.
 // Each CTA owns a slice of rows; reductions write per-CTA partial sums to a
-// double-buffered array, pass a grid barrier and are summed in CTA order by
-// every CTA (deterministic, identical in all CTAs).
+// double-buffered array, pass a grid barrier, and every CTA reads the partials
+// in parallel (one per thread) and adds them with the same fixed-order tree
+// (deterministic, identical in all CTAs).
 struct MgsArgs {
   int m, nvec, also;
   Z* x;
@@ -180,8 +181,8 @@ __device__ bool grid_sum(const MgsArgs& a, int& round, const double* v, int k, d
   if (!grid_barrier(a.bar, a.err, a.spin_limit)) return false;
   for (int t = 0; t < k; ++t) {
     double s = 0.0;
-    for (unsigned b = 0; b < gridDim.x; ++b) s += ((volatile double*)buf)[(size_t)b * 4 + t];
-    out[t] = s;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) s += ((volatile double*)buf)[(size_t)b * 4 + t];
+    out[t] = block_sum(s, sh);
   }
   return true;
 }
